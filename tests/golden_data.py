@@ -1,0 +1,71 @@
+"""Loads the committed golden fixtures (see tests/golden/make_golden.py).
+
+Synthetic data graphs are regenerated from their seeds by libpsm_gen and
+checked against the SHA-256 recorded when the fixtures were made.
+"""
+from __future__ import annotations
+
+import gzip
+import hashlib
+import json
+from functools import lru_cache
+from pathlib import Path
+
+import numpy as np
+
+from psm_benchmark_b200 import gen
+from psm_benchmark_b200.graphs import Graph
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def graph_sha(g: Graph) -> str:
+    h = hashlib.sha256()
+    for a in (g.off, g.nbr, g.labels):
+        h.update(np.ascontiguousarray(a, np.uint32).tobytes())
+    return h.hexdigest()
+
+
+@lru_cache(maxsize=1)
+def golden():
+    with gzip.open(GOLDEN / "golden_ref.json.gz", "rt") as f:
+        return json.load(f)
+
+
+@lru_cache(maxsize=1)
+def hprd():
+    """(graph, [10 queries], recorded counts) of the reference's HPRD-15 set."""
+    z = np.load(GOLDEN / "hprd15.npz")
+    g = Graph(off=z["off"], nbr=z["nbr"], labels=z["labels"])
+    qs = []
+    for lab, e in zip(z["q_labels"], z["q_edges"]):
+        e = e[e[:, 0] >= 0]
+        qs.append(Graph.from_edges(len(lab), lab, e))
+    return g, qs, [int(x) for x in z["recorded_counts"]]
+
+
+def query_from_rec(rec) -> Graph:
+    return Graph.from_edges(len(rec["labels"]), rec["labels"], rec["edges"])
+
+
+@lru_cache(maxsize=4)
+def synthetic_graph(name: str) -> Graph:
+    case = next(c for c in golden()["synthetic"] if c["name"] == name)
+    spec = case["spec"]
+    if spec["kind"] == "plain_small":
+        g = gen.make_graph("chung_lu", 1, n=9460, num_labels=307, zipf_s=1.1)
+    else:
+        g = gen.make_graph("rmat", spec["index"], scale=spec["scale"], edge_factor=spec["edge_factor"],
+                           num_labels=spec["num_labels"])
+    if graph_sha(g) != case["sha256"]:
+        raise AssertionError(f"generator drift: {name} graph hash changed")
+    return g
+
+
+def synthetic_cases():
+    for case in golden()["synthetic"]:
+        yield case["name"], case
+
+
+def tables_of(d):
+    return {(a, b): (np.array(off, np.uint32), np.array(adj, np.uint32)) for a, b, off, adj in d["tables"]}
