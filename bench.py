@@ -1,0 +1,330 @@
+"""Benchmark of the subgraph-matching hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (plain method, larger graph): an R-MAT data graph (scale 20 =
+1,048,576 vertices, a=.57 b=c=.19, edge factor 8, ~8.0M undirected edges
+after symmetrising and dedup) with 32 uniform labels, and 200 random-walk
+queries (100 of 12 and 100 of 16 vertices, half sparse / half dense), CFL
+filter + CFL order, embedding counts capped at 1e9, one query per launch
+sequence. Synthetic data generated from fixed seeds (no dataset download).
+
+One step = the 200 queries through the plain path. `value` is queries/s
+from the device time of the launches (CUDA events on the library's stream,
+graph resident in HBM); `e2e` is the same through the C ABI call psm_match
+with host query buffers, host->device descriptor copies and device->host
+result reads inside the wall-clock timed region. The data graph (72 MB) fits
+in L2, so L2 is flushed (256 MiB write) before every timed step. With N GPUs
+each rank runs the whole workload on its own replica of the graph (replicas
+only, weak scaling); times are the max over ranks.
+
+--impl reference times the reference's own CPU implementation (the
+SubgraphMatching.out binary built from the reference sources by
+oracle/Makefile) on the host cores, per query with -threadnums = all cores,
+on a bounded sample of the same queries per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "queries/sec (plain GPU path, CFL_CFL_EXPLORE, cap 1e9)"
+WORKLOAD = "plain_rmat_s20"
+REF_BIN = ROOT / "oracle" / "_ref" / "SubgraphMatching.out"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the
+    timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap")
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([x.strip() for x in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+        return self
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and "Active" in r[3 + i]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_workload(args):
+    from psm_benchmark_b200 import gen
+    return gen.plain_rmat(num_queries=args.queries, scale=args.scale)
+
+
+# --------------------------------------------------------------- reference --
+
+def ref_available():
+    return REF_BIN.exists() and os.access(REF_BIN, os.X_OK)
+
+
+def run_reference_query(data_txt, qpath, threads, cap, tmp: Path, time_limit=600):
+    log = tmp / "ref.log"
+    if log.exists():
+        log.unlink()
+    cmd = [str(REF_BIN), "-d", data_txt, "-q", qpath, "-threadnums", str(threads),
+           "-num", str(cap) if cap else "MAX", "-time_limit", str(time_limit), "-OutputFile", str(log),
+           "-QorCandi", "C", "-split", "linear", "-schedule", "busy2idlenostop", "-BackMethods", "CFL_CFL_EXPLORE"]
+    subprocess.run(cmd, check=True, capture_output=True, timeout=time_limit + 120)
+    text = log.read_text()
+    total = float(re.findall(r"Total time \(seconds\): ([0-9.e+-]+)", text)[-1])
+    count = int(re.findall(r"#Embeddings: (\d+)", text)[-1])
+    over = int(re.findall(r"Overtime: (\d+)", text)[-1])
+    return total, count, over
+
+
+class ReferenceRunner:
+    """Writes the workload in the reference's text format once and runs the
+    reference binary per query."""
+
+    def __init__(self, w):
+        from psm_benchmark_b200 import gen
+        self.tmp = Path(tempfile.mkdtemp(prefix="psmref_"))
+        d = self.tmp / "d1" / "d2"
+        d.mkdir(parents=True)
+        self.data_txt = str(d / "graph.txt")
+        gen.write_text(w.graph, self.data_txt)
+        qd = self.tmp / "q1" / "q2" / "q3"
+        qd.mkdir(parents=True)
+        self.qpaths = []
+        for i, q in enumerate(w.queries):
+            p = qd / f"q{i}.txt"
+            q.write_text(p)
+            self.qpaths.append(str(p))
+        self.cap = w.cap
+
+    def sample(self, threads, budget_s, start=0):
+        """Runs queries from `start` (cyclic) until `budget_s` of reference
+        "Total time" has accumulated; returns (n, total_s, counts)."""
+        n, tot, counts = 0, 0.0, []
+        i = start
+        while tot < budget_s and n < len(self.qpaths):
+            t, c, over = run_reference_query(self.data_txt, self.qpaths[i % len(self.qpaths)], threads, self.cap,
+                                             self.tmp)
+            n += 1
+            tot += t
+            counts.append(c)
+            i += 1
+        return n, tot, counts
+
+
+def cpu_info():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    if not ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference binary oracle/_ref/SubgraphMatching.out "
+                                                              "was not built (reference sources absent at build)"}))
+        return
+    w = make_workload(args)
+    rr = ReferenceRunner(w)
+    cores = os.cpu_count() or 1
+    for i in range(args.warmup):
+        rr.sample(cores, 0.5, start=i)
+    per_step = []
+    nq = 0
+    t0 = time.time()
+    for s in range(args.steps):
+        n, tot, _ = rr.sample(cores, args.ref_budget, start=s * 7)
+        per_step.append(tot / max(n, 1))
+        nq += n
+    wall = time.time() - t0
+    sec_per_query = float(np.mean(per_step))
+    value = 1.0 / sec_per_query
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_query * 1e3 * len(w.queries),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "queries_per_step": len(w.queries), "method": "CFL_CFL_EXPLORE",
+                       "cap": w.cap},
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "reference",
+                             "sample": f"{nq} queries of the workload over {args.steps} steps (about "
+                                       f"{args.ref_budget:.0f} s of reference Total time per step), "
+                                       f"-threadnums {cores}, CPU {cpu_info()}",
+                             "wall_s": wall},
+            "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# -------------------------------------------------------------------- ours --
+
+def flush_l2(buf):
+    buf.add_(1)
+
+
+def ours_arm(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from psm_benchmark_b200 import api
+    w = make_workload(args)
+    eng = api.Engine(device=local, arena_bytes=args.arena_gb << 30)
+    dg = api.DataGraph.from_graph(w.graph)
+    flush = torch.empty(256 << 20 >> 2, dtype=torch.float32, device=f"cuda:{local}")
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def step():
+        res = []
+        for q in w.queries:
+            res.append(api.match(eng, dg, q, w.method, cap=w.cap, time_limit=args.time_limit))
+        return res
+
+    for _ in range(args.warmup):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        step()
+    clocks = ClockSampler(local).start()
+    barrier()
+    dev_ms = 0.0
+    enum_ms = 0.0
+    alg = 0
+    h2d = d2h = 0
+    counts = None
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        res = step()
+        dev_ms += sum(r.prep_ms + r.enum_ms for r in res)
+        enum_ms += sum(r.enum_ms for r in res)
+        alg += sum(r.alg_bytes for r in res)
+        h2d += sum(r.h2d_bytes for r in res)
+        d2h += sum(r.d2h_bytes for r in res)
+        counts = [r.count for r in res]
+        bad = [r.status for r in res if r.status not in (0,)]
+        if bad:
+            raise SystemExit(f"query failures: {bad[:5]}")
+    barrier()
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    if dist is not None:
+        t = torch.tensor([dev_ms, wall], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms, wall = float(t[0]), float(t[1])
+    nq = len(w.queries)
+    value = world * nq * args.steps / (dev_ms / 1e3)
+    e2e = world * nq * args.steps / wall
+    hbm, peak_kind = peaks()
+    achieved = alg / (enum_ms / 1e3) / 1e9 if enum_ms > 0 else 0.0
+    line = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "graph": "R-MAT scale 20, edge factor 8, 32 uniform labels",
+                       "vertices": w.graph.num_vertices, "edges": w.graph.num_edges,
+                       "queries_per_step": nq, "query_sizes": "100 x 12, 100 x 16", "method": w.method,
+                       "cap": w.cap, "parallelism": f"replicas x{world}",
+                       "l2": "flushed (256 MiB write) before every step; 72 MB graph L2-resident within a step"},
+            "embeddings_per_s": world * sum(counts) * args.steps / (dev_ms / 1e3),
+            "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps},
+            "gpu_launches": (5 if True else 0) * nq * args.steps,
+            "roofline": {"bound": "hbm", "kernel": "enum_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None},
+            "clocks": clk}
+    if rank == 0 and args.cpu_baseline and ref_available():
+        rr = ReferenceRunner(w)
+        cores = os.cpu_count() or 1
+        n, tot, _ = rr.sample(cores, args.ref_budget)
+        line["cpu_baseline"] = {"value": n / tot, "unit": "queries/s", "cores": cores, "kind": "reference",
+                                "sample": f"first {n} queries of the workload (~{args.ref_budget:.0f} s of reference "
+                                          f"Total time), -threadnums {cores}, CPU {cpu_info()}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--queries", type=int, default=200)
+    ap.add_argument("--scale", type=int, default=20)
+    ap.add_argument("--time-limit", type=float, default=600.0)
+    ap.add_argument("--arena-gb", type=int, default=8)
+    ap.add_argument("--ref-budget", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+    else:
+        ours_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,136 @@
+/*
+ * psm_b200.h - C ABI of the B200 (sm_100a) subgraph-matching engine.
+ *
+ * Drop-in for the hot path of PSM_Benchmark (reference project), which has
+ * no plugin registry: its boundary is the static C++ API that
+ * matching/StudyPerformance.cpp drives and the SubgraphMatching.out command
+ * line. Each entry point below names the reference interface it replaces.
+ * Plain pointers and sizes only; every call returns a psm_status; nothing
+ * throws across the boundary. A context owns one CUDA stream and one device
+ * arena; calls on one context must not overlap (use one context per host
+ * thread), graphs may be shared by contexts on the same device.
+ */
+#ifndef PSM_B200_H
+#define PSM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum psm_status {
+    PSM_OK = 0,
+    PSM_ERR_ARG = 1,      /* invalid argument / unsupported query          */
+    PSM_ERR_OOM = 2,      /* device arena or device memory exhausted        */
+    PSM_ERR_TIMEOUT = 3,  /* time limit hit: counts are partial (Overtime 1) */
+    PSM_ERR_CUDA = 4,     /* CUDA runtime error, or no usable sm_100 device */
+    PSM_ERR_IO = 5,       /* file could not be read                         */
+    PSM_ERR_INTERNAL = 9  /* a device-side wait gave up / invariant broken  */
+} psm_status;
+
+enum { PSM_FILTER_NLF = 0, PSM_FILTER_GQL = 1, PSM_FILTER_CFL = 2 };
+enum { PSM_ORDER_GQL = 0, PSM_ORDER_CFL = 1 };
+/* Engines of the reference. All count the same embeddings; every engine is
+ * served by the one set-intersection enumerator. */
+enum { PSM_ENGINE_LFTJ = 0, PSM_ENGINE_GQL = 1, PSM_ENGINE_EXPLORE = 2 };
+
+#define PSM_MAX_QUERY_VERTICES 32
+
+typedef struct psm_graph psm_graph;
+typedef struct psm_context psm_context;
+typedef struct psm_run psm_run;
+
+/* A query graph: labels[num_vertices], undirected edges as pairs
+ * (edges[2i], edges[2i+1]), vertex ids 0..num_vertices-1. Must be connected
+ * and simple, with at most PSM_MAX_QUERY_VERTICES vertices. */
+typedef struct psm_query_desc {
+    uint32_t num_vertices;
+    uint32_t num_edges;
+    const uint32_t* labels;
+    const uint32_t* edges;
+} psm_query_desc;
+
+typedef struct psm_options {
+    uint32_t filter;          /* PSM_FILTER_*  (-BackMethods field 1) */
+    uint32_t order;           /* PSM_ORDER_*   (field 2)              */
+    uint32_t engine;          /* PSM_ENGINE_*  (field 3)              */
+    uint32_t emit;            /* 1: also materialise embeddings       */
+    uint64_t cap;             /* -num; 0 = no cap (MAX)               */
+    double time_limit_s;      /* -time_limit; <= 0 means 60           */
+    uint64_t emit_capacity;   /* rows of embeddings kept when emit=1  */
+} psm_options;
+
+typedef struct psm_result {
+    uint64_t count;           /* #Embeddings = min(total, cap)                  */
+    uint64_t calls;           /* extension candidates examined                  */
+    uint64_t memory_bytes;    /* candidates + tables, computeMemoryCostInBytes */
+    uint64_t table_entries;   /* entries over all candidate-edge tables         */
+    uint64_t alg_bytes;       /* algorithmic bytes read by the intersections    */
+    uint64_t donations;       /* work-stealing donations during enumeration     */
+    uint32_t overtime;        /* 1 if the time limit was hit                    */
+    uint32_t filter_ok;       /* 0 if a candidate set came out empty            */
+    uint32_t status;          /* psm_status of this query                       */
+    uint32_t reserved;
+    double prep_ms;           /* device time of filter + tables + order         */
+    double enum_ms;           /* device time of the enumeration                 */
+    uint64_t h2d_bytes;       /* host->device bytes of the call (its share)     */
+    uint64_t d2h_bytes;       /* device->host bytes of the call (its share)     */
+} psm_result;
+
+const char* psm_status_string(int status);
+/* Message of the last failing call on this thread ("" if none). */
+const char* psm_last_error(void);
+/* Library / device banner, e.g. for the CLI log. */
+const char* psm_version(void);
+
+/* ---- data graph (replaces Graph::loadGraphFromFile, graph/graph.cpp:92-172,
+ *      and the label index / NLF built by graph.cpp:15-52) ---- */
+int psm_graph_from_csr(const uint32_t* offsets, const uint32_t* neighbors, const uint32_t* labels,
+                       uint32_t num_vertices, psm_graph** out);
+int psm_graph_load(const char* path, psm_graph** out); /* reference text format */
+int psm_graph_info(const psm_graph* g, uint32_t* num_vertices, uint64_t* num_edges, uint32_t* num_labels,
+                   uint32_t* max_degree, uint32_t* max_label_frequency);
+void psm_graph_free(psm_graph* g);
+
+/* ---- execution context: stream + device arena ---- */
+int psm_context_create(int device, uint64_t arena_bytes, psm_context** out);
+void psm_context_free(psm_context* ctx);
+
+/* ---- plain path: one query on the whole GPU (replaces the per-query body of
+ *      split_C_test, matching/StudyPerformance.cpp:1150-1781: FilterVertices::
+ *      {NLF,GQL,CFL}Filter + sortCandidates, BuildTable::buildTables,
+ *      GenerateQueryPlan::generate{GQL,CFL}QueryPlan, EvaluateQuery::
+ *      ParallelExecute with the LFTJ/GQL/EXPLORE engine) ---- */
+int psm_match(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
+              psm_result* res);
+
+/* Same as psm_match but keeps the query's device state for inspection until
+ * psm_run_free (one live run per context). */
+int psm_run_create(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
+                   psm_run** out, psm_result* res);
+/* Sorted candidate set of query vertex u in original data ids
+ * (the reference's candidates[u] after sortCandidates). */
+int psm_run_candidates(psm_run* run, uint32_t u, uint32_t* buf, uint32_t buf_len, uint32_t* n);
+/* Candidate-edge table T[a][b] (the reference's Edges edge_matrix[a][b]):
+ * offsets[rows+1] and entries[nnz], positions into candidates of b. */
+int psm_run_table(psm_run* run, uint32_t a, uint32_t b, uint32_t* offsets, uint32_t offsets_len,
+                  uint32_t* entries, uint32_t entries_len, uint32_t* rows, uint32_t* nnz);
+/* Matching order and pivots (UnitArgs::order / pivots). */
+int psm_run_order(psm_run* run, uint32_t* order, uint32_t* pivot);
+/* Embeddings of an emit run: rows of num_vertices original ids, indexed by
+ * query vertex. */
+int psm_run_embeddings(psm_run* run, uint32_t* buf, uint64_t buf_rows, uint64_t* rows);
+void psm_run_free(psm_run* run);
+
+/* ---- batched path: many queries through one persistent preparation launch
+ *      and one persistent enumeration launch (no counterpart in the
+ *      reference, which runs queries one process at a time) ---- */
+int psm_match_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, uint32_t nq,
+                    const psm_options* opt, psm_result* results);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

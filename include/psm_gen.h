@@ -56,6 +56,11 @@ int psmgen_query(const uint32_t* off, const uint32_t* nbr, const uint32_t* label
                  uint32_t* q_labels, uint32_t* edges, uint32_t max_edges,
                  uint32_t* num_edges, uint32_t* data_ids);
 
+/* Writes the graph in the reference's text format ("t V E", "v id label
+ * degree", "e u v" with u < v). Returns 0 on success. */
+int psmgen_write_text(const uint32_t* off, const uint32_t* nbr, const uint32_t* labels, uint32_t num_vertices,
+                      const char* path);
+
 void psmgen_free(void* p);
 
 #ifdef __cplusplus

@@ -1,0 +1,436 @@
+// C ABI implementation (include/psm_b200.h): contexts, device arena layout,
+// kernel sequencing for the plain and batched paths, result read-back.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "host.h"
+
+int psm_graph_build(const uint32_t* off, const uint32_t* nbr, const uint32_t* labels, uint32_t V, psm_graph** out,
+                    std::string* err);
+int psm_graph_parse(const char* path, psm_graph** out, std::string* err);
+void psm_graph_destroy(psm_graph* g);
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(e == cudaErrorMemoryAllocation ? PSM_ERR_OOM : PSM_ERR_CUDA,
+                std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                              \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);   \
+    } while (0)
+
+constexpr size_t ALIGN = 256;
+inline size_t align_up(size_t x, size_t a = ALIGN) { return (x + a - 1) / a * a; }
+
+// Host-side bump allocator over the device arena.
+struct Bump {
+    char* base;
+    size_t top, cap;
+    template <class T>
+    T* take(size_t count) {
+        size_t bytes = align_up(std::max<size_t>(count, 1) * sizeof(T));
+        if (top + bytes > cap) return nullptr;
+        T* p = (T*)(base + top);
+        top += bytes;
+        return p;
+    }
+};
+
+}  // namespace
+
+struct psm_context {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    char* arena = nullptr;
+    size_t arena_bytes = 0;
+    size_t fixed_bytes = 0;       // permanent region at the start of the arena
+    DevArena* d_devarena = nullptr;
+    void* d_barrier = nullptr;
+    u32* d_ticket = nullptr;
+    void* d_enum_scratch = nullptr;
+    int prep_threads = 512;
+    int prep_grid_blocks = 0;
+    int prep_block_blocks = 0;
+    int enum_blocks = 0;
+    cudaEvent_t ev[4]{};
+    std::vector<char> host_stage;  // QDesc / QState staging
+    bool run_live = false;
+};
+
+struct psm_run {
+    psm_context* ctx = nullptr;
+    const psm_graph* g = nullptr;
+    QState* d_q = nullptr;
+    QState hq{};
+    QDesc* hdesc = nullptr;  // host copy (order / labels)
+    u32 n = 0;
+};
+
+namespace {
+
+struct Layout {
+    QDesc* d_desc;
+    QState* d_q;
+    u32* d_prefix;
+    DevResult* d_res;
+};
+
+// Per-query device buffers and QState initialisation.
+int setup_query(psm_context* ctx, const psm_graph& g, const QDesc& d, const psm_options& opt, Bump& b,
+                QDesc* d_desc, u32 scan_words, QState& q) {
+    memset(&q, 0, sizeof(q));
+    q.desc = d_desc;
+    u32 maxw = 1, maxb = 1;
+    for (u32 u = 0; u < d.n; ++u) {
+        u32 B = g.freq(d.label[u]);
+        u32 W = (B + 31) / 32;
+        q.bwords[u] = W;
+        q.bm[u] = b.take<u32>(W);
+        q.rank[u] = b.take<u32>(W);
+        q.list[u] = b.take<u32>(B);
+        if (!q.bm[u] || !q.rank[u] || !q.list[u]) return fail(PSM_ERR_OOM, "device arena exhausted (candidates)");
+        maxw = std::max(maxw, W);
+        maxb = std::max(maxb, B);
+    }
+    u64 rows = 0;
+    for (u32 x = 0; x < d.n; ++x) rows += (u64)g.freq(d.label[x]) * (d.e_first[x + 1] - d.e_first[x]);
+    if (rows >= 0xFFFFFFF0ull) return fail(PSM_ERR_ARG, "candidate tables too large for 32-bit offsets");
+    q.acc = b.take<u32>(maxw);
+    q.tmp = b.take<u32>(maxw);
+    q.P = b.take<u32>(rows + 1);
+    q.scan = b.take<u32>(scan_words);
+    if (d.order == PSM_ORDER_CFL) {
+        q.est_a = b.take<u64>(maxb);
+        q.est_b = b.take<u64>(maxb);
+        q.est_out = b.take<u64>(PSM_PLAN_WORDS);
+        if (!q.est_a || !q.est_b || !q.est_out) return fail(PSM_ERR_OOM, "device arena exhausted (estimates)");
+    }
+    if (!q.acc || !q.tmp || !q.P || !q.scan) return fail(PSM_ERR_OOM, "device arena exhausted (tables)");
+    q.cap = opt.cap;
+    if (opt.emit) {
+        q.emit_cap_rows = opt.emit_capacity;
+        q.emit_buf = b.take<u32>((size_t)opt.emit_capacity * d.n);
+        if (!q.emit_buf) return fail(PSM_ERR_OOM, "device arena exhausted (embeddings)");
+    }
+    return PSM_OK;
+}
+
+u64 budget_ns(const psm_options& o) {
+    double s = o.time_limit_s > 0 ? o.time_limit_s : 60.0;
+    return (u64)(s * 1e9);
+}
+
+void fill_result(const DevResult& r, float prep_ms, float enum_ms, u64 donations, psm_result* out) {
+    out->count = r.count;
+    out->calls = r.calls;
+    out->memory_bytes = r.memory_bytes;
+    out->table_entries = r.table_nnz;
+    out->alg_bytes = r.alg_bytes;
+    out->donations = donations;
+    out->overtime = r.overtime;
+    out->filter_ok = r.filter_ok;
+    out->status = r.status == PSM_DEV_OK ? (r.overtime ? PSM_ERR_TIMEOUT : PSM_OK)
+                                         : (r.status == PSM_DEV_OOM ? PSM_ERR_OOM : PSM_ERR_INTERNAL);
+    out->reserved = 0;
+    out->prep_ms = prep_ms;
+    out->enum_ms = enum_ms;
+}
+
+// Runs nq queries. grid_team: prepare the (single) query with the whole grid
+// (plain path); otherwise one block per query (batched path).
+int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, u32 nq, const psm_options& opt,
+                bool grid_team, psm_result* results, psm_run* keep) {
+    if (!ctx || !g || !qs || nq == 0) return fail(PSM_ERR_ARG, "null argument");
+    if (ctx->run_live) return fail(PSM_ERR_ARG, "a psm_run is still alive on this context");
+    CK(cudaSetDevice(ctx->device));
+    Bump b{ctx->arena, ctx->fixed_bytes, ctx->arena_bytes};
+    // descriptors
+    std::vector<QDesc> descs(nq);
+    std::string err;
+    for (u32 i = 0; i < nq; ++i) {
+        int rc = psm_build_qdesc(*g, qs[i], opt, &descs[i], &err);
+        if (rc) return fail(rc, "query " + std::to_string(i) + ": " + err);
+    }
+    Layout lay;
+    lay.d_desc = b.take<QDesc>(nq);
+    lay.d_q = b.take<QState>(nq);
+    lay.d_prefix = b.take<u32>(nq + 1);
+    lay.d_res = b.take<DevResult>(nq);
+    if (!lay.d_desc || !lay.d_q || !lay.d_prefix || !lay.d_res) return fail(PSM_ERR_OOM, "device arena exhausted");
+    const u32 scan_words = grid_team ? (u32)ctx->prep_grid_blocks + 1 : 2u;
+    std::vector<QState> hq(nq);
+    for (u32 i = 0; i < nq; ++i) {
+        int rc = setup_query(ctx, *g, descs[i], opt, b, lay.d_desc + i, scan_words, hq[i]);
+        if (rc) return rc;
+    }
+    // the rest of the arena is the device-side allocator region (tables)
+    DevArena da{};
+    size_t start = align_up(b.top);
+    if (start + 4096 > b.cap) return fail(PSM_ERR_OOM, "device arena exhausted (no table space)");
+    da.base = (u32*)(ctx->arena + start);
+    da.top = 0;
+    da.cap = (b.cap - start) / sizeof(u32);
+    // uploads: descriptors (used prefix only), states, allocator, barrier
+    for (u32 i = 0; i < nq; ++i)
+        CK(cudaMemcpyAsync(lay.d_desc + i, &descs[i], psm_qdesc_bytes(descs[i]), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(lay.d_q, hq.data(), sizeof(QState) * nq, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_devarena, &da, sizeof(da), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemsetAsync(ctx->d_barrier, 0, 64, ctx->st));
+    CK(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), ctx->st));
+    const u64 budget = budget_ns(opt);
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    if (grid_team) {
+        CK(psm_launch_prep_grid(g->dev, lay.d_q, ctx->d_barrier, ctx->d_devarena, budget, ctx->prep_grid_blocks,
+                                ctx->prep_threads, ctx->st));
+    } else {
+        int blocks = std::min<int>(ctx->prep_block_blocks, (int)nq);
+        CK(psm_launch_prep_block(g->dev, lay.d_q, nq, ctx->d_ticket, ctx->d_devarena, blocks, ctx->prep_threads,
+                                 ctx->st));
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_prefix, budget, opt.emit ? 1 : 0,
+                       ctx->enum_blocks, ctx->st));
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(psm_launch_gather(lay.d_q, nq, lay.d_res, ctx->st));
+    std::vector<DevResult> res(nq);
+    CK(cudaMemcpyAsync(res.data(), lay.d_res, sizeof(DevResult) * nq, cudaMemcpyDeviceToHost, ctx->st));
+    u32 enum_err = 0;
+    u64 donations = 0;
+    CK(psm_enum_read_ctl(ctx->d_enum_scratch, &enum_err, &donations, ctx->st));
+    float prep_ms = 0, enum_ms = 0;
+    CK(cudaEventElapsedTime(&prep_ms, ctx->ev[0], ctx->ev[1]));
+    CK(cudaEventElapsedTime(&enum_ms, ctx->ev[1], ctx->ev[2]));
+    u64 h2d = sizeof(QState) * (u64)nq + sizeof(DevArena) + 64 + 4, d2h = sizeof(DevResult) * (u64)nq + 64;
+    for (u32 i = 0; i < nq; ++i) h2d += psm_qdesc_bytes(descs[i]);
+    int worst = PSM_OK;
+    for (u32 i = 0; i < nq; ++i) {
+        fill_result(res[i], prep_ms, enum_ms, donations, &results[i]);
+        results[i].h2d_bytes = h2d / nq;
+        results[i].d2h_bytes = d2h / nq;
+        if (enum_err) results[i].status = PSM_ERR_INTERNAL;
+        if (results[i].status != PSM_OK && worst == PSM_OK) worst = (int)results[i].status;
+    }
+    if (grid_team) {
+        u32 ab = 0;
+        CK(cudaMemcpy(&ab, (char*)ctx->d_barrier + 8, sizeof(u32), cudaMemcpyDeviceToHost));
+        if (ab) {
+            for (u32 i = 0; i < nq; ++i) results[i].status = PSM_ERR_INTERNAL;
+            worst = PSM_ERR_INTERNAL;
+        }
+    }
+    if (keep) {
+        keep->ctx = ctx;
+        keep->g = g;
+        keep->d_q = lay.d_q;
+        CK(cudaMemcpy(&keep->hq, lay.d_q, sizeof(QState), cudaMemcpyDeviceToHost));
+        keep->hdesc = new QDesc;
+        memcpy(keep->hdesc, &descs[0], sizeof(QDesc));
+        keep->n = descs[0].n;
+        ctx->run_live = true;
+    }
+    if (worst == PSM_ERR_INTERNAL) return fail(worst, enum_err ? "enumeration wait gave up" : "device error");
+    if (worst == PSM_ERR_OOM) return fail(worst, "device arena exhausted (tables)");
+    if (worst == PSM_ERR_TIMEOUT) return fail(worst, "time limit reached");
+    return PSM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* psm_status_string(int s) {
+    switch (s) {
+        case PSM_OK: return "ok";
+        case PSM_ERR_ARG: return "invalid argument";
+        case PSM_ERR_OOM: return "out of device memory";
+        case PSM_ERR_TIMEOUT: return "time limit reached";
+        case PSM_ERR_CUDA: return "CUDA error";
+        case PSM_ERR_IO: return "I/O error";
+        case PSM_ERR_INTERNAL: return "internal error";
+        default: return "unknown status";
+    }
+}
+
+const char* psm_last_error(void) { return g_last_error.c_str(); }
+
+const char* psm_version(void) { return "psm_b200 1.0 (sm_100a)"; }
+
+int psm_graph_from_csr(const uint32_t* off, const uint32_t* nbr, const uint32_t* labels, uint32_t V, psm_graph** out) {
+    if (!out) return fail(PSM_ERR_ARG, "null out");
+    std::string err;
+    int rc = psm_graph_build(off, nbr, labels, V, out, &err);
+    return rc ? fail(rc, err) : PSM_OK;
+}
+
+int psm_graph_load(const char* path, psm_graph** out) {
+    if (!path || !out) return fail(PSM_ERR_ARG, "null argument");
+    std::string err;
+    int rc = psm_graph_parse(path, out, &err);
+    return rc ? fail(rc, err) : PSM_OK;
+}
+
+int psm_graph_info(const psm_graph* g, uint32_t* V, uint64_t* E, uint32_t* L, uint32_t* maxdeg, uint32_t* maxfreq) {
+    if (!g) return fail(PSM_ERR_ARG, "null graph");
+    if (V) *V = g->V;
+    if (E) *E = g->nnz / 2;
+    if (L) *L = g->L;
+    if (maxdeg) *maxdeg = g->max_degree;
+    if (maxfreq) *maxfreq = g->max_label_freq;
+    return PSM_OK;
+}
+
+void psm_graph_free(psm_graph* g) { psm_graph_destroy(g); }
+
+int psm_context_create(int device, uint64_t arena_bytes, psm_context** out) {
+    if (!out) return fail(PSM_ERR_ARG, "null out");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PSM_ERR_CUDA, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(PSM_ERR_ARG, "bad device index");
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(PSM_ERR_CUDA, "this build targets sm_100a (B200) only");
+    CK(cudaSetDevice(device));
+    auto* c = new psm_context;
+    c->device = device;
+    if (arena_bytes == 0) arena_bytes = 4ull << 30;
+    c->arena_bytes = arena_bytes;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&c->arena, arena_bytes);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    if (e != cudaSuccess) {
+        psm_context_free(c);
+        return cuda_fail(e, "context allocation");
+    }
+    Bump b{c->arena, 0, arena_bytes};
+    c->d_devarena = b.take<DevArena>(1);
+    c->d_barrier = b.take<char>(64);
+    c->d_ticket = b.take<u32>(1);
+    c->d_enum_scratch = b.take<char>(psm_enum_scratch_bytes());
+    c->fixed_bytes = b.top;
+    if (psm_prep_grid_max_blocks(c->prep_threads, &c->prep_grid_blocks) != cudaSuccess ||
+        psm_enum_max_blocks(&c->enum_blocks) != cudaSuccess) {
+        psm_context_free(c);
+        return fail(PSM_ERR_CUDA, "occupancy query failed");
+    }
+    c->prep_block_blocks = prop.multiProcessorCount * 4;
+    *out = c;
+    return PSM_OK;
+}
+
+void psm_context_free(psm_context* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    if (c->arena) cudaFree(c->arena);
+    if (c->st) cudaStreamDestroy(c->st);
+    delete c;
+}
+
+int psm_match(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
+              psm_result* res) {
+    if (!opt || !res) return fail(PSM_ERR_ARG, "null argument");
+    return run_queries(ctx, g, q, 1, *opt, true, res, nullptr);
+}
+
+int psm_match_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, uint32_t nq,
+                    const psm_options* opt, psm_result* results) {
+    if (!opt || !results) return fail(PSM_ERR_ARG, "null argument");
+    return run_queries(ctx, g, qs, nq, *opt, false, results, nullptr);
+}
+
+int psm_run_create(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
+                   psm_run** out, psm_result* res) {
+    if (!opt || !res || !out) return fail(PSM_ERR_ARG, "null argument");
+    auto* r = new psm_run;
+    int rc = run_queries(ctx, g, q, 1, *opt, true, res, r);
+    if (r->ctx == nullptr) {
+        delete r;
+        *out = nullptr;
+        return rc;
+    }
+    *out = r;
+    return rc;
+}
+
+int psm_run_candidates(psm_run* r, uint32_t u, uint32_t* buf, uint32_t buf_len, uint32_t* n) {
+    if (!r || !n || u >= r->n) return fail(PSM_ERR_ARG, "bad run / vertex");
+    u32 c = r->hq.cnt[u];
+    *n = c;
+    if (!buf) return PSM_OK;
+    if (buf_len < c) return fail(PSM_ERR_ARG, "buffer too small");
+    std::vector<u32> tmp(c);
+    if (c) CK(cudaMemcpy(tmp.data(), r->hq.list[u], c * sizeof(u32), cudaMemcpyDeviceToHost));
+    for (u32 i = 0; i < c; ++i) buf[i] = r->g->orig[tmp[i]];
+    return PSM_OK;
+}
+
+int psm_run_table(psm_run* r, uint32_t a, uint32_t b, uint32_t* offsets, uint32_t offsets_len, uint32_t* entries,
+                  uint32_t entries_len, uint32_t* rows, uint32_t* nnz) {
+    if (!r || a >= r->n || b >= r->n) return fail(PSM_ERR_ARG, "bad run / vertices");
+    const QDesc& d = *r->hdesc;
+    if (!((d.adj[a] >> b) & 1u)) return fail(PSM_ERR_ARG, "not a query edge");
+    if (r->hq.adj == nullptr) return fail(PSM_ERR_ARG, "tables were not built (empty candidate set)");
+    u32 e = d.e_first[a] + (u32)__builtin_popcount(d.adj[a] & ((1u << b) - 1u));
+    u32 base = r->hq.e_row_base[e], R = r->hq.cnt[a];
+    std::vector<u32> P(R + 1);
+    CK(cudaMemcpy(P.data(), r->hq.P + base, (R + 1) * sizeof(u32), cudaMemcpyDeviceToHost));
+    u32 z = P[R] - P[0];
+    if (rows) *rows = R;
+    if (nnz) *nnz = z;
+    if (offsets) {
+        if (offsets_len < R + 1) return fail(PSM_ERR_ARG, "offsets buffer too small");
+        for (u32 i = 0; i <= R; ++i) offsets[i] = P[i] - P[0];
+    }
+    if (entries) {
+        if (entries_len < z) return fail(PSM_ERR_ARG, "entries buffer too small");
+        if (z) CK(cudaMemcpy(entries, r->hq.adj + P[0], z * sizeof(u32), cudaMemcpyDeviceToHost));
+    }
+    return PSM_OK;
+}
+
+int psm_run_order(psm_run* r, uint32_t* order, uint32_t* pivot) {
+    if (!r) return fail(PSM_ERR_ARG, "null run");
+    for (u32 i = 0; i < r->n; ++i) {
+        if (order) order[i] = r->hq.order[i];
+        if (pivot) pivot[i] = r->hq.pivot[i];
+    }
+    return PSM_OK;
+}
+
+int psm_run_embeddings(psm_run* r, uint32_t* buf, uint64_t buf_rows, uint64_t* rows) {
+    if (!r || !rows) return fail(PSM_ERR_ARG, "null argument");
+    u64 have = std::min<u64>(r->hq.emit_rows, r->hq.emit_cap_rows);
+    *rows = have;
+    if (!buf || have == 0) return PSM_OK;
+    if (buf_rows < have) return fail(PSM_ERR_ARG, "buffer too small");
+    CK(cudaMemcpy(buf, r->hq.emit_buf, have * r->n * sizeof(u32), cudaMemcpyDeviceToHost));
+    return PSM_OK;
+}
+
+void psm_run_free(psm_run* r) {
+    if (!r) return;
+    if (r->ctx) r->ctx->run_live = false;
+    delete r->hdesc;
+    delete r;
+}
+
+}  // extern "C"

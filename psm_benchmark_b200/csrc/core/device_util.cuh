@@ -1,0 +1,87 @@
+// Small device helpers shared by the preparation and enumeration kernels.
+#pragma once
+#include <stdint.h>
+
+#include "psm_internal.h"
+
+#define FULL_MASK 0xffffffffu
+
+__device__ __forceinline__ u32 lane_id() { return threadIdx.x & 31u; }
+
+// First index i in [lo, hi) with a[i] >= key (hi if none).
+__device__ __forceinline__ u32 lower_bound_u32(const u32* __restrict__ a, u32 lo, u32 hi, u32 key) {
+    while (lo < hi) {
+        u32 mid = (lo + hi) >> 1;
+        if (__ldg(a + mid) < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// True if key occurs in the ascending range a[lo, hi).
+__device__ __forceinline__ bool contains_u32(const u32* __restrict__ a, u32 lo, u32 hi, u32 key) {
+    u32 i = lower_bound_u32(a, lo, hi, key);
+    return i < hi && __ldg(a + i) == key;
+}
+
+// Range of neighbours of internal vertex v that carry label l.
+__device__ __forceinline__ void label_run(const DevGraph& g, u32 v, u32 l, u32& s, u32& e) {
+    u32 lo = g.off[v], hi = g.off[v + 1];
+    if (l >= g.L) {
+        s = e = lo;
+        return;
+    }
+    s = lower_bound_u32(g.nbr, lo, hi, g.lab_off[l]);
+    e = lower_bound_u32(g.nbr, s, hi, g.lab_off[l + 1]);
+}
+
+__device__ __forceinline__ bool test_bit(const u32* bm, u32 pos) { return (bm[pos >> 5] >> (pos & 31)) & 1u; }
+
+__device__ __forceinline__ u32 warp_sum(u32 x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL_MASK, x, o);
+    return x;
+}
+__device__ __forceinline__ u64 warp_sum64(u64 x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(FULL_MASK, x, o);
+    return x;
+}
+__device__ __forceinline__ u32 warp_max(u32 x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x = max(x, __shfl_xor_sync(FULL_MASK, x, o));
+    return x;
+}
+// Inclusive warp prefix sum.
+__device__ __forceinline__ u32 warp_incl_scan(u32 x) {
+    u32 lane = lane_id();
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        u32 y = __shfl_up_sync(FULL_MASK, x, o);
+        if (lane >= (u32)o) x += y;
+    }
+    return x;
+}
+
+__device__ __forceinline__ u64 global_timer_ns() {
+    u64 t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ u32 ld_acquire_u32(const u32* p) {
+    u32 v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(u32* p, u32 v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ u64 ld_acquire_u64(const u64* p) {
+    u64 v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ u32 ld_volatile_u32(const u32* p) { return *(const volatile u32*)p; }

@@ -1,0 +1,45 @@
+// Host-side runtime types (not part of the C ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "psm_b200.h"
+#include "psm_internal.h"
+
+struct psm_graph {
+    int device = 0;
+    u32 V = 0, L = 0;
+    u64 nnz = 0;
+    u32 max_degree = 0, max_label_freq = 0;
+    std::vector<u32> lab_off;      // host copy of the bucket ranges
+    std::vector<u32> to_internal;  // original id -> internal id
+    std::vector<u32> orig;         // internal id -> original id
+    u32* d_off = nullptr;
+    u32* d_nbr = nullptr;
+    u32* d_lab_off = nullptr;
+    u32* d_orig = nullptr;
+    DevGraph dev{};
+    u32 freq(u32 l) const { return l < L ? lab_off[l + 1] - lab_off[l] : 0u; }
+};
+
+// Builds the device query descriptor (validation, NLF lists, CFL plans).
+// Returns PSM_OK or PSM_ERR_ARG with *err set.
+int psm_build_qdesc(const psm_graph& g, const psm_query_desc& q, const psm_options& opt, QDesc* d, std::string* err);
+
+// Size in bytes of the prefix of a QDesc that must be copied to the device.
+size_t psm_qdesc_bytes(const QDesc& d);
+
+// Kernel launchers (prep.cu, enum.cu).
+cudaError_t psm_launch_prep_block(const DevGraph& g, QState* qs, u32 nq, u32* ticket, DevArena* arena, int blocks,
+                                  int threads, cudaStream_t st);
+cudaError_t psm_launch_prep_grid(const DevGraph& g, QState* qs, void* barrier, DevArena* arena, u64 budget_ns,
+                                 int blocks, int threads, cudaStream_t st);
+cudaError_t psm_prep_grid_max_blocks(int threads, int* blocks);
+size_t psm_enum_scratch_bytes();
+cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, u32* prefix, u64 budget_ns,
+                            int emit, int blocks, cudaStream_t st);
+cudaError_t psm_enum_max_blocks(int* blocks);
+cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st);
+cudaError_t psm_enum_read_ctl(void* scratch, u32* error, u64* donations, cudaStream_t st);

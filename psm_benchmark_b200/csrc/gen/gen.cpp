@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <random>
@@ -283,6 +284,34 @@ int psmgen_query(const uint32_t* off, const uint32_t* nbr, const uint32_t* label
     }
     *num_edges = (uint32_t)chosen.size();
     return 0;
+}
+
+int psmgen_write_text(const uint32_t* off, const uint32_t* nbr, const uint32_t* labels, uint32_t n,
+                      const char* path) {
+    FILE* f = fopen(path, "wb");
+    if (!f) return 1;
+    std::vector<char> buf;
+    buf.reserve(1 << 22);
+    char tmp[64];
+    auto flush = [&]() {
+        if (!buf.empty()) fwrite(buf.data(), 1, buf.size(), f);
+        buf.clear();
+    };
+    auto put = [&](const char* s, int len) {
+        buf.insert(buf.end(), s, s + len);
+        if (buf.size() > (1u << 22)) flush();
+    };
+    uint64_t m = 0;
+    for (uint32_t v = 0; v < n; ++v)
+        for (uint32_t j = off[v]; j < off[v + 1]; ++j) m += nbr[j] > v;
+    put(tmp, snprintf(tmp, sizeof(tmp), "t %u %llu\n", n, (unsigned long long)m));
+    for (uint32_t v = 0; v < n; ++v)
+        put(tmp, snprintf(tmp, sizeof(tmp), "v %u %u %u\n", v, labels[v], off[v + 1] - off[v]));
+    for (uint32_t v = 0; v < n; ++v)
+        for (uint32_t j = off[v]; j < off[v + 1]; ++j)
+            if (nbr[j] > v) put(tmp, snprintf(tmp, sizeof(tmp), "e %u %u\n", v, nbr[j]));
+    flush();
+    return fclose(f) == 0 ? 0 : 2;
 }
 
 void psmgen_free(void* p) { free(p); }

@@ -54,6 +54,8 @@ def _lib():
     lib.psmgen_query.argtypes = [u32p, u32p, u32p, C.c_uint32, C.c_uint32, C.c_int, C.c_uint64,
                                  u32p, u32p, C.c_uint32, u32p, u32p]
     lib.psmgen_free.argtypes = [C.c_void_p]
+    lib.psmgen_write_text.argtypes = [u32p, u32p, u32p, C.c_uint32, C.c_char_p]
+    lib.psmgen_write_text.restype = C.c_int
     for f in (lib.psmgen_chung_lu, lib.psmgen_rmat, lib.psmgen_labels, lib.psmgen_query):
         f.restype = C.c_int
     return lib
@@ -111,6 +113,16 @@ def query(g: Graph, k: int, dense: bool, seed: int) -> Graph:
         raise RuntimeError(f"psmgen_query failed ({rc})")
     m = int(ne[0])
     return Graph.from_edges(k, ql, edges[: 2 * m].reshape(-1, 2))
+
+
+def write_text(g: Graph, path) -> None:
+    """Fast writer of the reference text format (same output as Graph.write_text)."""
+    off = np.ascontiguousarray(g.off, np.uint32)
+    nbr = np.ascontiguousarray(g.nbr, np.uint32)
+    lab = np.ascontiguousarray(g.labels, np.uint32)
+    rc = _lib().psmgen_write_text(_u32p(off), _u32p(nbr), _u32p(lab), g.num_vertices, str(path).encode())
+    if rc:
+        raise RuntimeError(f"psmgen_write_text failed ({rc})")
 
 
 BASE_SEED = 0x50534D00

@@ -1,0 +1,107 @@
+"""ctypes binding of libpsm_b200.so (the C ABI in include/psm_b200.h).
+
+There is no fallback: if the library is missing or cannot reach an sm_100
+device, calls raise PsmError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from functools import lru_cache
+from pathlib import Path
+
+_PKG = Path(__file__).resolve().parent
+LIB_PATH = _PKG / "libpsm_b200.so"
+
+PSM_OK, PSM_ERR_ARG, PSM_ERR_OOM, PSM_ERR_TIMEOUT, PSM_ERR_CUDA, PSM_ERR_IO, PSM_ERR_INTERNAL = 0, 1, 2, 3, 4, 5, 9
+FILTERS = {"NLF": 0, "GQL": 1, "CFL": 2}
+ORDERS = {"GQL": 0, "CFL": 1}
+ENGINES = {"LFTJ": 0, "GQL": 1, "EXPLORE": 2}
+
+EXPORTS = [
+    "psm_status_string", "psm_last_error", "psm_version",
+    "psm_graph_from_csr", "psm_graph_load", "psm_graph_info", "psm_graph_free",
+    "psm_context_create", "psm_context_free",
+    "psm_match", "psm_run_create", "psm_run_candidates", "psm_run_table", "psm_run_order",
+    "psm_run_embeddings", "psm_run_free", "psm_match_batch",
+]
+
+
+class PsmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"psm error {code}: {msg}")
+        self.code = code
+
+
+class QueryDesc(C.Structure):
+    _fields_ = [("num_vertices", C.c_uint32), ("num_edges", C.c_uint32),
+                ("labels", C.POINTER(C.c_uint32)), ("edges", C.POINTER(C.c_uint32))]
+
+
+class Options(C.Structure):
+    _fields_ = [("filter", C.c_uint32), ("order", C.c_uint32), ("engine", C.c_uint32), ("emit", C.c_uint32),
+                ("cap", C.c_uint64), ("time_limit_s", C.c_double), ("emit_capacity", C.c_uint64)]
+
+
+class Result(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("calls", C.c_uint64), ("memory_bytes", C.c_uint64),
+                ("table_entries", C.c_uint64), ("alg_bytes", C.c_uint64), ("donations", C.c_uint64),
+                ("overtime", C.c_uint32), ("filter_ok", C.c_uint32), ("status", C.c_uint32),
+                ("reserved", C.c_uint32), ("prep_ms", C.c_double), ("enum_ms", C.c_double),
+                ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+@lru_cache(maxsize=1)
+def lib():
+    if not LIB_PATH.exists():
+        raise PsmError(PSM_ERR_CUDA, f"{LIB_PATH} is not built (python -m psm_benchmark_b200.build)")
+    L = C.CDLL(str(LIB_PATH))
+    u32p = C.POINTER(C.c_uint32)
+    vp = C.c_void_p
+    sig = {
+        "psm_status_string": ([C.c_int], C.c_char_p),
+        "psm_last_error": ([], C.c_char_p),
+        "psm_version": ([], C.c_char_p),
+        "psm_graph_from_csr": ([u32p, u32p, u32p, C.c_uint32, C.POINTER(vp)], C.c_int),
+        "psm_graph_load": ([C.c_char_p, C.POINTER(vp)], C.c_int),
+        "psm_graph_info": ([vp, u32p, C.POINTER(C.c_uint64), u32p, u32p, u32p], C.c_int),
+        "psm_graph_free": ([vp], None),
+        "psm_context_create": ([C.c_int, C.c_uint64, C.POINTER(vp)], C.c_int),
+        "psm_context_free": ([vp], None),
+        "psm_match": ([vp, vp, C.POINTER(QueryDesc), C.POINTER(Options), C.POINTER(Result)], C.c_int),
+        "psm_run_create": ([vp, vp, C.POINTER(QueryDesc), C.POINTER(Options), C.POINTER(vp), C.POINTER(Result)],
+                           C.c_int),
+        "psm_run_candidates": ([vp, C.c_uint32, u32p, C.c_uint32, u32p], C.c_int),
+        "psm_run_table": ([vp, C.c_uint32, C.c_uint32, u32p, C.c_uint32, u32p, C.c_uint32, u32p, u32p], C.c_int),
+        "psm_run_order": ([vp, u32p, u32p], C.c_int),
+        "psm_run_embeddings": ([vp, u32p, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
+        "psm_run_free": ([vp], None),
+        "psm_match_batch": ([vp, vp, C.POINTER(QueryDesc), C.c_uint32, C.POINTER(Options), C.POINTER(Result)],
+                            C.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    return L
+
+
+def check(rc: int, allow=()):
+    if rc != PSM_OK and rc not in allow:
+        raise PsmError(rc, lib().psm_last_error().decode())
+    return rc
+
+
+def parse_method(method: str):
+    """'CFL_CFL_EXPLORE' -> (filter, order, engine) codes (-BackMethods triple,
+    matching/StudyPerformance.cpp:1013-1030)."""
+    parts = method.split("_")
+    if len(parts) != 3:
+        raise PsmError(PSM_ERR_ARG, f"method must be FILTER_ORDER_ENGINE, got {method!r}")
+    f, o, e = parts
+    if f not in FILTERS or o not in ORDERS or e not in ENGINES:
+        raise PsmError(PSM_ERR_ARG, f"unsupported method {method!r} (filters NLF/GQL/CFL, orders GQL/CFL, "
+                                    "engines GQL/EXPLORE/LFTJ)")
+    return FILTERS[f], ORDERS[o], ENGINES[e]

@@ -1,0 +1,117 @@
+"""Parity of the sm_100a path with the reference, through the C ABI.
+
+Candidate sets, candidate-edge tables, matching orders, memory cost and
+embedding counts must be identical (bit-exact integer results) to what the
+reference computes: its recorded HPRD counts and the fixtures dumped from the
+reference's own code (tests/golden), plus the oracle restatement on extra
+cases."""
+import numpy as np
+import pytest
+
+from psm_benchmark_b200 import api
+from oracle.oracle import OracleGraph
+from tests import golden_data as gd
+from tests.gpu_common import check_run_against_dump, engine  # noqa: F401
+
+pytestmark = pytest.mark.gpu
+
+METHODS = {"GQL_GQL": "GQL_GQL_GQL", "CFL_CFL": "CFL_CFL_EXPLORE", "NLF_GQL": "NLF_GQL_LFTJ"}
+
+
+@pytest.fixture(scope="module")
+def hprd_dev():
+    g, qs, counts = gd.hprd()
+    return api.DataGraph.from_graph(g), qs, counts
+
+
+@pytest.mark.parametrize("qi", range(1, 11))
+@pytest.mark.parametrize("m", list(METHODS))
+def test_hprd(engine, hprd_dev, qi, m):
+    dg, qs, counts = hprd_dev
+    with api.Run(engine, dg, qs[qi - 1], METHODS[m]) as run:
+        assert run.result.count == counts[qi - 1]
+        assert run.result.status == 0
+        check_run_against_dump(run, gd.golden()["hprd"]["dumps"][f"{qi}:{m}"])
+
+
+@pytest.mark.parametrize("name", [n for n, _ in gd.synthetic_cases()])
+def test_synthetic_against_reference(engine, name):
+    case = dict(gd.synthetic_cases())[name]
+    dg = api.DataGraph.from_graph(gd.synthetic_graph(name))
+    for j, entry in enumerate(case["queries"]):
+        q = gd.query_from_rec(entry["query"])
+        for m, d in entry["methods"].items():
+            with api.Run(engine, dg, q, m, cap=entry["cap"]) as run:
+                assert run.result.count == d["count"], (name, j, m)
+                check_run_against_dump(run, d)
+
+
+def test_batch_equals_plain(engine):
+    """Per-query counts of the batched path equal the plain path's."""
+    name = "rmat12"
+    case = dict(gd.synthetic_cases())[name]
+    dg = api.DataGraph.from_graph(gd.synthetic_graph(name))
+    qs = [gd.query_from_rec(e["query"]) for e in case["queries"]]
+    caps = [e["cap"] for e in case["queries"]]
+    for m in ("CFL_CFL_EXPLORE", "GQL_GQL_GQL"):
+        plain = [api.match(engine, dg, q, m, cap=c).count for q, c in zip(qs, caps)]
+        ref = [e["methods"][m]["count"] for e in case["queries"]]
+        assert plain == ref
+        # one batch per cap value (the cap is a per-launch option)
+        for c in sorted(set(caps)):
+            idx = [i for i, x in enumerate(caps) if x == c]
+            batch = [r.count for r in api.match_batch(engine, dg, [qs[i] for i in idx], m, cap=c)]
+            assert batch == [plain[i] for i in idx]
+
+
+def test_embeddings_match_oracle(engine):
+    """Full embedding sets of small queries."""
+    g = gd.synthetic_graph("rmat12")
+    og = OracleGraph(g)
+    dg = api.DataGraph.from_graph(g)
+    case = dict(gd.synthetic_cases())["rmat12"]
+    checked = 0
+    for entry in case["queries"]:
+        q = gd.query_from_rec(entry["query"])
+        ref = og.run(q, "CFL", "CFL", emit_limit=200000)
+        if ref.count > 200000 or ref.count == 0:
+            continue
+        with api.Run(engine, dg, q, "CFL_CFL_EXPLORE", emit=ref.count + 10) as run:
+            got = run.embeddings()
+        assert got.shape[0] == ref.count
+        assert set(map(tuple, got.tolist())) == set(map(tuple, ref.embeddings.tolist()))
+        checked += 1
+    assert checked >= 5
+
+
+def test_edge_cases(engine):
+    from psm_benchmark_b200.graphs import Graph
+    g = gd.synthetic_graph("rmat12")
+    og = OracleGraph(g)
+    dg = api.DataGraph.from_graph(g)
+    l0 = int(g.labels[0])
+    cases = [
+        Graph.from_edges(1, [l0], []),                              # single vertex
+        Graph.from_edges(2, [l0, l0], [(0, 1)]),                    # one edge, same labels
+        Graph.from_edges(3, [l0, 10**6, l0], [(0, 1), (1, 2)]),     # label absent from the data graph
+        Graph.from_edges(4, [l0, l0, l0, l0], [(0, 1), (1, 2), (2, 3), (3, 0)]),
+    ]
+    for q in cases:
+        for m in ("CFL_CFL_EXPLORE", "GQL_GQL_GQL"):
+            f, o, _ = m.split("_")
+            ref = og.run(q, f, o, cap=10**6, want_tables=False)
+            got = api.match(engine, dg, q, m, cap=10**6)
+            assert got.count == ref.count, (q.labels, m)
+
+
+def test_cap_is_exact(engine):
+    """With a cap the count is min(total, cap) exactly."""
+    from psm_benchmark_b200.graphs import Graph
+    g = gd.synthetic_graph("rmat12")
+    dg = api.DataGraph.from_graph(g)
+    l0 = int(g.labels[0])
+    star = Graph.from_edges(4, [l0, l0, l0, l0], [(0, 1), (0, 2), (0, 3)])
+    full = api.match(engine, dg, star, "CFL_CFL_EXPLORE").count
+    assert full > 1000
+    for cap in (1, 7, 999, full - 1, full, full + 5):
+        assert api.match(engine, dg, star, "CFL_CFL_EXPLORE", cap=cap).count == min(full, cap)
