@@ -77,6 +77,8 @@ typedef struct psm_result {
     double enum_ms;           /* device time of the enumeration                 */
     uint64_t h2d_bytes;       /* host->device bytes of the call (its share)     */
     uint64_t d2h_bytes;       /* device->host bytes of the call (its share)     */
+    uint64_t tasks;           /* enumeration tasks run (launch-wide)            */
+    uint64_t idle_polls;      /* polls of idle warps waiting for work           */
 } psm_result;
 
 const char* psm_status_string(int status);

@@ -89,7 +89,7 @@ namespace {
 struct Layout {
     QDesc* d_desc;
     QState* d_q;
-    u32* d_prefix;
+    char* d_enum_q;  // per-query enumeration scratch
     DevResult* d_res;
 };
 
@@ -172,9 +172,9 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     Layout lay;
     lay.d_desc = b.take<QDesc>(nq);
     lay.d_q = b.take<QState>(nq);
-    lay.d_prefix = b.take<u32>(nq + 1);
+    lay.d_enum_q = b.take<char>(psm_enum_query_bytes(nq));
     lay.d_res = b.take<DevResult>(nq);
-    if (!lay.d_desc || !lay.d_q || !lay.d_prefix || !lay.d_res) return fail(PSM_ERR_OOM, "device arena exhausted");
+    if (!lay.d_desc || !lay.d_q || !lay.d_enum_q || !lay.d_res) return fail(PSM_ERR_OOM, "device arena exhausted");
     const u32 scan_words = grid_team ? (u32)ctx->prep_grid_blocks + 1 : 2u;
     std::vector<QState> hq(nq);
     for (u32 i = 0; i < nq; ++i) {
@@ -206,15 +206,15 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
                                  ctx->st));
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_prefix, budget, opt.emit ? 1 : 0,
+    CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_enum_q, budget, opt.emit ? 1 : 0,
                        ctx->enum_blocks, ctx->st));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     CK(psm_launch_gather(lay.d_q, nq, lay.d_res, ctx->st));
     std::vector<DevResult> res(nq);
     CK(cudaMemcpyAsync(res.data(), lay.d_res, sizeof(DevResult) * nq, cudaMemcpyDeviceToHost, ctx->st));
-    u32 enum_err = 0;
-    u64 donations = 0;
-    CK(psm_enum_read_ctl(ctx->d_enum_scratch, &enum_err, &donations, ctx->st));
+    EnumStats es{};
+    CK(psm_enum_read_ctl(ctx->d_enum_scratch, &es, ctx->st));
+    const u32 enum_err = es.error;
     float prep_ms = 0, enum_ms = 0;
     CK(cudaEventElapsedTime(&prep_ms, ctx->ev[0], ctx->ev[1]));
     CK(cudaEventElapsedTime(&enum_ms, ctx->ev[1], ctx->ev[2]));
@@ -222,7 +222,9 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     for (u32 i = 0; i < nq; ++i) h2d += psm_qdesc_bytes(descs[i]);
     int worst = PSM_OK;
     for (u32 i = 0; i < nq; ++i) {
-        fill_result(res[i], prep_ms, enum_ms, donations, &results[i]);
+        fill_result(res[i], prep_ms, enum_ms, es.donations, &results[i]);
+        results[i].tasks = es.tasks;
+        results[i].idle_polls = es.idle_polls;
         results[i].h2d_bytes = h2d / nq;
         results[i].d2h_bytes = d2h / nq;
         if (enum_err) results[i].status = PSM_ERR_INTERNAL;

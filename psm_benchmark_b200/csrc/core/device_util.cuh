@@ -85,3 +85,12 @@ __device__ __forceinline__ u64 ld_acquire_u64(const u64* p) {
     return v;
 }
 __device__ __forceinline__ u32 ld_volatile_u32(const u32* p) { return *(const volatile u32*)p; }
+
+// Volatile load by lane 0, broadcast to the warp: every lane sees the same
+// value, so branches on it keep the warp converged (full-mask warp
+// primitives after a branch on a per-lane volatile read are undefined).
+__device__ __forceinline__ u32 warp_ld_volatile_u32(const u32* p) {
+    u32 v = 0;
+    if ((threadIdx.x & 31u) == 0) v = *(const volatile u32*)p;
+    return __shfl_sync(0xffffffffu, v, 0);
+}

@@ -16,16 +16,19 @@
 //  - candidates are generated 32 at a time: lane i takes element i of the
 //    shortest backward-neighbour row (the "driver"), binary-searches it in
 //    the other rows and checks it against same-label earlier vertices; a
-//    ballot compacts the survivors. The last depth is only counted (row
-//    length directly when a single row has no possible collision);
-//  - work: root candidates of all queries of a launch are handed out by an
-//    atomic ticket; an idle warp raises a "hungry" counter and busy warps
-//    donate the upper half of the unexplored driver range at their
-//    shallowest depth to a bounded lock-free queue (the reference's
-//    "linear" split, TaskPool.cpp:1407-1424);
-//  - termination: a pending-work counter (root pool + live tasks) reaches
-//    zero. Every wait is bounded by a deadline and an iteration cap; on
-//    expiry the kernel records an error and returns.
+//    ballot compacts the survivors. The last two depths are fused: each lane
+//    takes one candidate of depth n-2 and counts its completions itself;
+//  - initial work: the edges of the first candidate-edge table (pairs of
+//    depth-0 / depth-1 candidates) of every query of the launch, handed out
+//    in chunks by one atomic ticket; queries of up to three vertices hand out
+//    root candidates instead;
+//  - load balance: an idle warp raises a "hungry" counter; while more warps
+//    are hungry than tasks are queued, busy warps donate the upper half of
+//    their shallowest unexplored range (the reference's "linear" split,
+//    TaskPool.cpp:1407-1424) to a bounded lock-free queue;
+//  - termination: a pending-work counter (the initial pool + live tasks)
+//    reaches zero. Every wait is bounded by a deadline and an iteration cap;
+//    on expiry the kernel records an error and returns.
 #include <cuda_runtime.h>
 
 #include "device_util.cuh"
@@ -33,14 +36,19 @@
 
 namespace {
 
-constexpr u32 QCAP = 4096;          // steal queue slots
-constexpr u32 TASK_WORDS = 5 + PSM_MAXQ;
+constexpr u32 QCAP = 4096;     // steal queue slots
+constexpr u32 HDR_WORDS = 6;   // kind, qi, d0, b, e, drv
+constexpr u32 TASK_WORDS = HDR_WORDS + PSM_MAXQ;
 constexpr u32 WARPS_PER_BLOCK = 8;
-constexpr u32 FULL_LEVEL = 0xFFFFFFFFu;  // task range: the whole driver row of d0
 
-struct Task {
-    u32 qi, d0, b, e, drv;
-    u32 pos[PSM_MAXQ];
+enum : u32 {
+    KIND_RANGE = 0,  // driver range [b, e) at depth d0, prefix pos[0, d0)
+    KIND_FULL = 1,   // whole driver row of depth d0, prefix pos[0, d0)
+    KIND_EDGES = 2,  // edges [b, e) of the first table (absolute entry indices)
+};
+
+struct TaskHdr {
+    u32 kind, qi, d0, b, e, drv;
 };
 
 struct Slot {
@@ -51,8 +59,8 @@ struct Slot {
 }  // namespace
 
 struct EnumCtl {
-    u32 root_ticket;
-    u32 total_roots;
+    u32 ticket;         // next grab of the initial pool
+    u32 total_grabs;
     u32 hungry;
     u32 q_head;
     u32 q_tail;
@@ -62,6 +70,8 @@ struct EnumCtl {
     unsigned long long pending;
     u64 deadline_ns;
     u64 donations;
+    u64 tasks;
+    u64 idle_polls;
 };
 
 namespace {
@@ -77,6 +87,15 @@ struct WarpStack {
     u32 chunk[PSM_MAXQ][32];
 };
 
+// Per query, filled by enum_init_kernel: how the initial pool of a query is
+// cut into grabs.
+struct PoolInfo {
+    u32 kind;   // KIND_RANGE (roots) or KIND_EDGES
+    u32 units;  // roots or first-table edges
+    u32 grab;   // units per grab
+    u32 first;  // absolute index of unit 0 (edges: P[base])
+};
+
 __device__ __forceinline__ u32 row_lo(const QState& q, u32 d, u32 k, const u32* pos) {
     return q.P[q.bn_tab[d][k] + pos[q.bn_depth[d][k]]];
 }
@@ -84,8 +103,8 @@ __device__ __forceinline__ u32 row_hi(const QState& q, u32 d, u32 k, const u32* 
     return q.P[q.bn_tab[d][k] + pos[q.bn_depth[d][k]] + 1];
 }
 
-// Picks the shortest backward-neighbour row at depth d; returns its length
-// and range, and adds the algorithmic bytes of reading all rows.
+// Picks the shortest backward-neighbour row at depth d as the driver and
+// adds the algorithmic bytes of reading all rows.
 __device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws, u64& bytes) {
     const u32 nb = q.nbn[d];
     u32 best = 0, blen = 0xFFFFFFFFu, bs = 0;
@@ -97,6 +116,7 @@ __device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws
         if (len < blen) blen = len, best = k, bs = lo;
     }
     bytes += by;
+    __syncwarp();
     if (lane_id() == 0) {
         ws->drv[d] = best;
         ws->cur[d] = bs;
@@ -106,6 +126,15 @@ __device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws
     }
     __syncwarp();
     return blen;
+}
+
+// Position of data vertex v (same label as query vertex u) among the sorted
+// candidates of u, from u's bitmap and rank; 0xFFFFFFFF if not a candidate.
+__device__ __forceinline__ u32 cand_pos(const QState& q, u32 u, u32 v) {
+    const u32 b = v - q.cbase[u];
+    const u32 word = q.bm[u][b >> 5];
+    if (!((word >> (b & 31u)) & 1u)) return 0xFFFFFFFFu;
+    return q.rank[u][b >> 5] + __popc(word & ((1u << (b & 31u)) - 1u));
 }
 
 // One lane's candidate test at depth d for driver element p (a position in
@@ -130,7 +159,7 @@ __device__ __forceinline__ bool accept(const QState& q, u32 d, u32 p, const Warp
     return true;
 }
 
-// Counts the candidates of the last depth d given the prefix in ws.
+// Warp-level count of the candidates of the last depth d given the prefix.
 __device__ u64 count_last(const QState& q, u32 d, WarpStack* ws, u64& bytes, u64& calls) {
     const u32 lane = lane_id();
     const u32 u = q.order[d];
@@ -150,26 +179,15 @@ __device__ u64 count_last(const QState& q, u32 d, WarpStack* ws, u64& bytes, u64
     const u32 same = q.same_mask[d];
     if (nb == 1) {
         if (!same) return blen;
-        // Subtract used same-label vertices that occur in the row: the
-        // position of a vertex in C(u_d) comes from u_d's bitmap and rank.
+        // Subtract used same-label vertices whose position is in the row.
         u32 hit = 0;
         if ((same >> lane) & 1u) {
-            // position of the used vertex among C(u_d) (sorted list), then
-            // membership of that position in the row
-            u32 v = ws->vid[lane];
-            u32 lo = 0, hi = q.cnt[u];
-            while (lo < hi) {
-                u32 mid = (lo + hi) >> 1;
-                if (list_d[mid] < v)
-                    lo = mid + 1;
-                else
-                    hi = mid;
-            }
-            if (lo < q.cnt[u] && list_d[lo] == v) hit = contains_u32(q.adj, bs, bs + blen, lo) ? 1u : 0u;
+            u32 x = cand_pos(q, u, ws->vid[lane]);
+            hit = (x != 0xFFFFFFFFu && contains_u32(q.adj, bs, bs + blen, x)) ? 1u : 0u;
         }
-        u32 h = __popc(__ballot_sync(FULL_MASK, hit));
-        return blen - h;
+        return blen - __popc(__ballot_sync(FULL_MASK, hit));
     }
+    __syncwarp();
     if (lane == 0) ws->drv[d] = best;
     __syncwarp();
     u64 c = 0;
@@ -218,82 +236,6 @@ __device__ u64 emit_last(QState& q, const DevGraph& g, u32 d, WarpStack* ws, u64
     return c;
 }
 
-// Bounded lock-free MPMC ring (sequence numbers per slot).
-__device__ bool enqueue(EnumCtl* ctl, Slot* slots, const Task& t) {
-    const u32 lane = lane_id();
-    u32 slot_idx = 0;
-    int ok = 0;
-    if (lane == 0) {
-        u32 pos = ld_volatile_u32(&ctl->q_tail);
-        for (int it = 0; it < 64; ++it) {
-            Slot* s = slots + (pos % QCAP);
-            u32 seq = ld_acquire_u32(&s->seq);
-            int diff = (int)(seq - pos);
-            if (diff == 0) {
-                if (atomicCAS(&ctl->q_tail, pos, pos + 1) == pos) {
-                    ok = 1;
-                    slot_idx = pos;
-                    break;
-                }
-                pos = ld_volatile_u32(&ctl->q_tail);
-            } else if (diff < 0) {
-                break;  // full
-            } else {
-                pos = ld_volatile_u32(&ctl->q_tail);
-            }
-        }
-    }
-    ok = __shfl_sync(FULL_MASK, ok, 0);
-    if (!ok) return false;
-    slot_idx = __shfl_sync(FULL_MASK, slot_idx, 0);
-    Slot* s = slots + (slot_idx % QCAP);
-    const u32* src = (const u32*)&t;
-    for (u32 i = lane; i < TASK_WORDS; i += 32) s->w[i] = src[i];
-    __threadfence();
-    __syncwarp();
-    if (lane == 0) st_release_u32(&s->seq, slot_idx + 1);
-    return true;
-}
-
-__device__ bool dequeue(EnumCtl* ctl, Slot* slots, Task& t) {
-    const u32 lane = lane_id();
-    u32 slot_idx = 0;
-    int ok = 0;
-    if (lane == 0) {
-        u32 pos = ld_volatile_u32(&ctl->q_head);
-        for (int it = 0; it < 64; ++it) {
-            Slot* s = slots + (pos % QCAP);
-            u32 seq = ld_acquire_u32(&s->seq);
-            int diff = (int)(seq - (pos + 1));
-            if (diff == 0) {
-                if (atomicCAS(&ctl->q_head, pos, pos + 1) == pos) {
-                    ok = 1;
-                    slot_idx = pos;
-                    break;
-                }
-                pos = ld_volatile_u32(&ctl->q_head);
-            } else if (diff < 0) {
-                break;  // empty
-            } else {
-                pos = ld_volatile_u32(&ctl->q_head);
-            }
-        }
-    }
-    ok = __shfl_sync(FULL_MASK, ok, 0);
-    if (!ok) return false;
-    slot_idx = __shfl_sync(FULL_MASK, slot_idx, 0);
-    Slot* s = slots + (slot_idx % QCAP);
-    __threadfence();
-    u32* dst = (u32*)&t;
-    for (u32 i = 0; i < TASK_WORDS; ++i) dst[i] = ld_volatile_u32(&s->w[i]);
-    __syncwarp();
-    if (lane == 0) {
-        __threadfence();
-        st_release_u32(&s->seq, slot_idx + QCAP);
-    }
-    return true;
-}
-
 // Last-depth count for one lane: the lane's own candidate p (data vertex v)
 // sits at depth dl - 1, the rest of the prefix is shared in ws. Counts the
 // positions in the intersection of the backward-neighbour rows of depth dl
@@ -314,7 +256,6 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const Warp
     calls += blen;
     if (blen == 0) return 0;
     const u32 u = q.order[dl];
-    const u32* list = q.list[u];
     const u32 same = q.same_mask[dl];
     if (nb == 1) {
         u64 c = blen;
@@ -322,12 +263,12 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const Warp
         while (m) {
             const u32 j = __ffs(m) - 1;
             m &= m - 1;
-            const u32 vj = j == dp ? v : ws->vid[j];
-            const u32 x = lower_bound_u32(list, 0, q.cnt[u], vj);
-            if (x < q.cnt[u] && __ldg(list + x) == vj && contains_u32(q.adj, blo, bhi, x)) --c;
+            const u32 x = cand_pos(q, u, j == dp ? v : ws->vid[j]);
+            if (x != 0xFFFFFFFFu && contains_u32(q.adj, blo, bhi, x)) --c;
         }
         return c;
     }
+    const u32* list = q.list[u];
     u64 c = 0;
     for (u32 e = blo; e < bhi; ++e) {
         const u32 x = __ldg(q.adj + e);
@@ -352,67 +293,176 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const Warp
     return c;
 }
 
-// Every 16 warp steps: donate work when another warp is idle, publish the
-// local count (so a capped query stops close to its cap) and stop on the
-// cap or the time limit. Returns true when the task must stop.
-__device__ bool periodic(QState& q, const Task& t, WarpStack* ws, u32 d, u32 d0, u32 iter, u64& count, u64 flush_at,
-                         EnumCtl* ctl, Slot* slots) {
+// ---------------------------------------------------------------- queue --
+
+// Bounded lock-free MPMC ring with a sequence number per slot. Lane 0 claims
+// a slot; the warp copies the task words. A failed claim backs off and gives
+// up after a few tries (the caller keeps the work).
+__device__ bool enqueue(EnumCtl* ctl, Slot* slots, const TaskHdr& h, const WarpStack* ws, u32 npos, u32 extra_at,
+                        u32 extra_val) {
     const u32 lane = lane_id();
-    if (ld_volatile_u32(&ctl->hungry) > 0) {
-        // (a) upper half of the shallowest unexplored driver range of at
-        // least 64 elements, else (b) the last unexplored chunk entry of the
-        // shallowest depth below d, as a task starting one level deeper.
+    u32 slot_idx = 0;
+    int ok = 0;
+    if (lane == 0) {
+        u32 pos = ld_volatile_u32(&ctl->q_tail);
+        for (int it = 0; it < 8; ++it) {
+            Slot* s = slots + (pos % QCAP);
+            u32 seq = ld_acquire_u32(&s->seq);
+            int diff = (int)(seq - pos);
+            if (diff == 0) {
+                u32 prev = atomicCAS(&ctl->q_tail, pos, pos + 1);
+                if (prev == pos) {
+                    ok = 1;
+                    slot_idx = pos;
+                    break;
+                }
+                pos = prev;
+            } else if (diff < 0) {
+                break;  // full
+            } else {
+                pos = ld_volatile_u32(&ctl->q_tail);
+            }
+        }
+    }
+    ok = __shfl_sync(FULL_MASK, ok, 0);
+    if (!ok) return false;
+    slot_idx = __shfl_sync(FULL_MASK, slot_idx, 0);
+    Slot* s = slots + (slot_idx % QCAP);
+    if (lane < HDR_WORDS) {
+        const u32 hv[HDR_WORDS] = {h.kind, h.qi, h.d0, h.b, h.e, h.drv};
+        u32 val = 0;
+#pragma unroll
+        for (u32 i = 0; i < HDR_WORDS; ++i)
+            if (lane == i) val = hv[i];
+        s->w[lane] = val;
+    }
+    s->w[HDR_WORDS + lane] = lane == extra_at ? extra_val : (lane < npos ? ws->pos[lane] : 0u);
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release_u32(&s->seq, slot_idx + 1);
+    return true;
+}
+
+// Takes a task; its prefix positions go straight into ws->pos.
+__device__ bool dequeue(EnumCtl* ctl, Slot* slots, TaskHdr& h, WarpStack* ws) {
+    const u32 lane = lane_id();
+    u32 slot_idx = 0;
+    int ok = 0;
+    if (lane == 0) {
+        u32 pos = ld_volatile_u32(&ctl->q_head);
+        for (int it = 0; it < 4; ++it) {
+            Slot* s = slots + (pos % QCAP);
+            u32 seq = ld_acquire_u32(&s->seq);
+            int diff = (int)(seq - (pos + 1));
+            if (diff == 0) {
+                u32 prev = atomicCAS(&ctl->q_head, pos, pos + 1);
+                if (prev == pos) {
+                    ok = 1;
+                    slot_idx = pos;
+                    break;
+                }
+                pos = prev;
+                __nanosleep(32u << it);
+            } else if (diff < 0) {
+                break;  // empty
+            } else {
+                pos = ld_volatile_u32(&ctl->q_head);
+            }
+        }
+    }
+    ok = __shfl_sync(FULL_MASK, ok, 0);
+    if (!ok) return false;
+    slot_idx = __shfl_sync(FULL_MASK, slot_idx, 0);
+    Slot* s = slots + (slot_idx % QCAP);
+    __threadfence();
+    u32 hw = lane < HDR_WORDS ? ld_volatile_u32(&s->w[lane]) : 0u;
+    h.kind = __shfl_sync(FULL_MASK, hw, 0);
+    h.qi = __shfl_sync(FULL_MASK, hw, 1);
+    h.d0 = __shfl_sync(FULL_MASK, hw, 2);
+    h.b = __shfl_sync(FULL_MASK, hw, 3);
+    h.e = __shfl_sync(FULL_MASK, hw, 4);
+    h.drv = __shfl_sync(FULL_MASK, hw, 5);
+    ws->pos[lane] = ld_volatile_u32(&s->w[HDR_WORDS + lane]);
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) st_release_u32(&s->seq, slot_idx + QCAP);
+    return true;
+}
+
+// Hands the upper half of a range to the queue when more warps are hungry
+// than tasks are queued. Returns true if it donated (the range end moved).
+__device__ bool try_donate_range(EnumCtl* ctl, Slot* slots, u32 kind, u32 qi, u32 d0, u32 cur, u32& end, u32 drv,
+                                 const WarpStack* ws, u32 min_len) {
+    if (end - cur < min_len) return false;
+    const u32 hungry = warp_ld_volatile_u32(&ctl->hungry);
+    if (hungry == 0) return false;
+    const u32 qlen = warp_ld_volatile_u32(&ctl->q_tail) - warp_ld_volatile_u32(&ctl->q_head);
+    if (qlen >= hungry) return false;
+    const u32 lane = lane_id();
+    const u32 mid = cur + ((end - cur) >> 1);
+    TaskHdr h{kind, qi, d0, mid, end, drv};
+    if (lane == 0) atomicAdd(&ctl->pending, 1ull);
+    __threadfence();
+    __syncwarp();
+    if (enqueue(ctl, slots, h, ws, d0, 0xFFFFFFFFu, 0)) {
+        if (lane == 0) atomicAdd((unsigned long long*)&ctl->donations, 1ull);
+        end = mid;
+        return true;
+    }
+    if (lane == 0) atomicAdd(&ctl->pending, (unsigned long long)-1ll);
+    return false;
+}
+
+// Every 16 warp steps inside a search: donate work to hungry warps, publish
+// the local count (so a capped query stops close to its cap) and stop on the
+// cap or the time limit. Returns true when the search must stop.
+__device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 iter, u64& count, EnumCtl* ctl,
+                         Slot* slots) {
+    const u32 lane = lane_id();
+    if (warp_ld_volatile_u32(&ctl->hungry) > 0) {
+        // (a) upper half of the shallowest driver range with >= 64 unexplored
+        // elements, else (b) the last unexplored chunk entry of the
+        // shallowest depth below d, as a task one level deeper.
         u32 dd = d0;
         for (; dd <= d; ++dd)
             if (ws->end[dd] - ws->cur[dd] >= 64u) break;
-        u32 de = d0;
-        for (; de < d; ++de)
-            if (ws->cn[de] > ws->ci[de]) break;
-        Task nt;
-        nt.qi = t.qi;
-        bool have = false;
         if (dd <= d) {
-            const u32 c0 = ws->cur[dd], e0 = ws->end[dd];
-            nt.d0 = dd;
-            nt.b = c0 + ((e0 - c0) >> 1);
-            nt.e = e0;
-            nt.drv = ws->drv[dd];
-            for (u32 i = 0; i < PSM_MAXQ; ++i) nt.pos[i] = i < dd ? ws->pos[i] : 0;
-            have = true;
-        } else if (de < d) {
-            nt.d0 = de + 1;
-            nt.b = FULL_LEVEL;
-            nt.e = FULL_LEVEL;
-            nt.drv = 0;
-            for (u32 i = 0; i < PSM_MAXQ; ++i) nt.pos[i] = i < de ? ws->pos[i] : 0;
-            nt.pos[de] = ws->chunk[de][ws->cn[de] - 1];
-            have = true;
-        }
-        if (have) {
-            if (lane == 0) atomicAdd(&ctl->pending, 1ull);
-            __threadfence();
+            u32 end = ws->end[dd];
+            bool done = try_donate_range(ctl, slots, KIND_RANGE, qi, dd, ws->cur[dd], end, ws->drv[dd], ws, 64u);
             __syncwarp();
-            if (enqueue(ctl, slots, nt)) {
-                if (lane == 0) {
-                    if (nt.b != FULL_LEVEL)
-                        ws->end[dd] = nt.b;
-                    else
+            if (done && lane == 0) ws->end[dd] = end;
+            __syncwarp();
+        } else {
+            u32 de = d0;
+            for (; de < d; ++de)
+                if (ws->cn[de] > ws->ci[de]) break;
+            const u32 hungry = warp_ld_volatile_u32(&ctl->hungry);
+            const u32 qlen = warp_ld_volatile_u32(&ctl->q_tail) - warp_ld_volatile_u32(&ctl->q_head);
+            if (de < d && qlen < hungry) {
+                TaskHdr h{KIND_FULL, qi, de + 1, 0, 0, 0};
+                if (lane == 0) atomicAdd(&ctl->pending, 1ull);
+                __threadfence();
+                __syncwarp();
+                if (enqueue(ctl, slots, h, ws, de, de, ws->chunk[de][ws->cn[de] - 1])) {
+                    __syncwarp();
+                    if (lane == 0) {
                         ws->cn[de] -= 1;
-                    atomicAdd((unsigned long long*)&ctl->donations, 1ull);
+                        atomicAdd((unsigned long long*)&ctl->donations, 1ull);
+                    }
+                } else if (lane == 0) {
+                    atomicAdd(&ctl->pending, (unsigned long long)-1ll);
                 }
-            } else if (lane == 0) {
-                atomicAdd(&ctl->pending, (unsigned long long)-1ll);
+                __syncwarp();
             }
-            __syncwarp();
         }
     }
-    if (count >= flush_at && lane == 0) {
+    if (count >= (1ull << 16) && lane == 0) {
         unsigned long long old = atomicAdd((unsigned long long*)&q.count, count);
         if (q.cap && old + count >= q.cap) atomicExch(&q.stop, 1u);
         count = 0;
     }
     count = __shfl_sync(FULL_MASK, count, 0);
-    u32 stop = ld_volatile_u32(&q.stop);
+    u32 stop = warp_ld_volatile_u32(&q.stop);
     if (!stop && (iter & 255u) == 0 && global_timer_ns() > ctl->deadline_ns) {
         if (lane == 0) {
             atomicExch(&q.overtime, 1u);
@@ -423,121 +473,97 @@ __device__ bool periodic(QState& q, const Task& t, WarpStack* ws, u32 d, u32 d0,
     return __shfl_sync(FULL_MASK, stop, 0) != 0;
 }
 
-// Runs one task to completion (or until the query stops).
-__device__ void run_task(const DevGraph& g, QState* qs, const Task& t, WarpStack* ws, EnumCtl* ctl, Slot* slots,
-                         bool emit) {
+// Depth-first search below the prefix ws->pos[0, d0): the level d0 has been
+// set up (driver range in ws). Returns false if the query stopped.
+__device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws, EnumCtl* ctl, Slot* slots, bool emit,
+                    u64& count, u64& bytes, u64& calls, u32& iter) {
     const u32 lane = lane_id();
-    QState& q = qs[t.qi];
     const u32 n = q.desc->n;
-    const u32 d0 = t.d0;
-    if (ld_volatile_u32(&q.stop)) return;
-    u64 count = 0, bytes = 0, calls = 0;
-    // restore the prefix
-    if (lane < d0) {
-        ws->pos[lane] = t.pos[lane];
-        ws->vid[lane] = q.list[q.order[lane]][t.pos[lane]];
-    }
-    if (lane == 0) {
-        ws->cur[d0] = t.b;
-        ws->end[d0] = t.e;
-        ws->drv[d0] = t.drv;
-        ws->cn[d0] = 0;
-        ws->ci[d0] = 0;
-    }
-    __syncwarp();
-    if (n == 1) {  // single-vertex query: every root candidate is an embedding
-        count = t.e - t.b;
-        calls = count;
-        if (emit) {
-            for (u32 i = t.b + lane; i < t.e; i += 32) {
-                unsigned long long r = atomicAdd((unsigned long long*)&q.emit_rows, 1ull);
-                if (r < q.emit_cap_rows) q.emit_buf[r] = g.orig[q.list[q.order[0]][i]];
-            }
-        }
-    } else if (t.b == FULL_LEVEL && d0 + 1 == n) {
-        // donated entry whose children are the last depth
-        count += emit ? emit_last(q, g, d0, ws, bytes, calls) : count_last(q, d0, ws, bytes, calls);
-    } else {
-        u32 d = d0;
-        if (t.b == FULL_LEVEL) setup_level(q, d0, ws, bytes);
-        u32 iter = 0;
-        u64 bytes_l = 0, calls_l = 0;  // per-lane parts, summed at the end
-        const u64 flush_at = 1ull << 16;
-        while (true) {
-            if (d + 2 == n && !emit) {
-                // The last two depths fused: each lane takes one driver
-                // element of depth d and counts its completions at depth
-                // d + 1 on its own (32 partial embeddings per warp step).
-                if (ws->cur[d] < ws->end[d]) {
-                    const u32 cur = ws->cur[d], end = ws->end[d];
-                    const u32 idx = cur + lane;
-                    u64 c = 0;
-                    if (idx < end) {
-                        const u32* list_d = q.list[q.order[d]];
-                        u32 p = d == 0 ? idx : q.adj[idx];
-                        if (d == 0 || accept(q, d, p, ws, list_d))
-                            c = lane_last_count(q, d + 1, p, list_d[p], ws, bytes_l, calls_l);
-                    }
-                    count += warp_sum64(c);
-                    calls += min(32u, end - cur);
-                    __syncwarp();
-                    if (lane == 0) ws->cur[d] = min(end, cur + 32u);
-                    __syncwarp();
-                    if ((++iter & 15u) == 0 && periodic(q, t, ws, d, d0, iter, count, flush_at, ctl, slots)) break;
-                } else {
-                    if (d == d0) break;
-                    d -= 1;
-                }
-                continue;
-            }
-            if (ws->ci[d] < ws->cn[d]) {
-                const u32 p = ws->chunk[d][ws->ci[d]];
-                __syncwarp();
-                if (lane == 0) {
-                    ws->ci[d] += 1;
-                    ws->pos[d] = p;
-                    ws->vid[d] = q.list[q.order[d]][p];
-                }
-                __syncwarp();
-                if (d + 2 == n) {
-                    u64 c = emit ? emit_last(q, g, d + 1, ws, bytes, calls) : count_last(q, d + 1, ws, bytes, calls);
-                    count += c;
-                } else {
-                    d += 1;
-                    setup_level(q, d, ws, bytes);
-                }
-            } else if (ws->cur[d] < ws->end[d]) {
+    u32 d = d0;
+    u64 bytes_l = 0, calls_l = 0;  // per-lane parts, summed at the end
+    bool go = true;
+    while (true) {
+        if (d + 2 == n && !emit) {
+            // The last two depths fused: each lane takes one driver element
+            // of depth d and counts its completions at depth d + 1 on its own.
+            if (ws->cur[d] < ws->end[d]) {
                 const u32 cur = ws->cur[d], end = ws->end[d];
                 const u32 idx = cur + lane;
-                bool ok = false;
-                u32 p = 0;
-                if (d == 0) {
-                    p = idx;
-                    ok = idx < end;
-                } else if (idx < end) {
-                    p = q.adj[idx];
-                    ok = accept(q, d, p, ws, q.list[q.order[d]]);
+                u64 c = 0;
+                if (idx < end) {
+                    const u32* list_d = q.list[q.order[d]];
+                    u32 p = d == 0 ? idx : q.adj[idx];
+                    if (d == 0 || accept(q, d, p, ws, list_d))
+                        c = lane_last_count(q, d + 1, p, list_d[p], ws, bytes_l, calls_l);
                 }
-                u32 bal = __ballot_sync(FULL_MASK, ok);
-                if (ok) ws->chunk[d][__popc(bal & ((1u << lane) - 1u))] = p;
+                count += warp_sum64(c);
                 calls += min(32u, end - cur);
                 __syncwarp();
-                if (lane == 0) {
-                    ws->cn[d] = __popc(bal);
-                    ws->ci[d] = 0;
-                    ws->cur[d] = min(end, cur + 32u);
-                }
+                if (lane == 0) ws->cur[d] = min(end, cur + 32u);
                 __syncwarp();
-                if ((++iter & 15u) == 0 && periodic(q, t, ws, d, d0, iter, count, flush_at, ctl, slots)) break;
+                if ((++iter & 15u) == 0 && periodic(q, qi, ws, d, d0, iter, count, ctl, slots)) {
+                    go = false;
+                    break;
+                }
             } else {
                 if (d == d0) break;
                 d -= 1;
             }
+            continue;
         }
-        bytes += warp_sum64(bytes_l);
-        calls += warp_sum64(calls_l);
+        if (ws->ci[d] < ws->cn[d]) {
+            const u32 p = ws->chunk[d][ws->ci[d]];
+            __syncwarp();
+            if (lane == 0) {
+                ws->ci[d] += 1;
+                ws->pos[d] = p;
+                ws->vid[d] = q.list[q.order[d]][p];
+            }
+            __syncwarp();
+            if (d + 2 == n) {
+                count += emit ? emit_last(q, g, d + 1, ws, bytes, calls) : count_last(q, d + 1, ws, bytes, calls);
+            } else {
+                d += 1;
+                setup_level(q, d, ws, bytes);
+            }
+        } else if (ws->cur[d] < ws->end[d]) {
+            const u32 cur = ws->cur[d], end = ws->end[d];
+            const u32 idx = cur + lane;
+            bool ok = false;
+            u32 p = 0;
+            if (d == 0) {
+                p = idx;
+                ok = idx < end;
+            } else if (idx < end) {
+                p = q.adj[idx];
+                ok = accept(q, d, p, ws, q.list[q.order[d]]);
+            }
+            u32 bal = __ballot_sync(FULL_MASK, ok);
+            if (ok) ws->chunk[d][__popc(bal & ((1u << lane) - 1u))] = p;
+            calls += min(32u, end - cur);
+            __syncwarp();
+            if (lane == 0) {
+                ws->cn[d] = __popc(bal);
+                ws->ci[d] = 0;
+                ws->cur[d] = min(end, cur + 32u);
+            }
+            __syncwarp();
+            if ((++iter & 15u) == 0 && periodic(q, qi, ws, d, d0, iter, count, ctl, slots)) {
+                go = false;
+                break;
+            }
+        } else {
+            if (d == d0) break;
+            d -= 1;
+        }
     }
-    if (lane == 0) {
+    bytes += warp_sum64(bytes_l);
+    calls += warp_sum64(calls_l);
+    return go;
+}
+
+__device__ void publish(QState& q, u64 count, u64 bytes, u64 calls) {
+    if (lane_id() == 0) {
         if (count) {
             unsigned long long old = atomicAdd((unsigned long long*)&q.count, count);
             if (q.cap && old + count >= q.cap) atomicExch(&q.stop, 1u);
@@ -547,64 +573,157 @@ __device__ void run_task(const DevGraph& g, QState* qs, const Task& t, WarpStack
     }
 }
 
-// Root ticket -> (query, candidate range); prefix[i] = roots before query i.
-__device__ bool take_root(EnumCtl* ctl, const u32* prefix, QState* qs, Task& t, u32 grab) {
+// Runs one task (prefix positions already in ws->pos[0, d0)).
+__device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpStack* ws, EnumCtl* ctl, Slot* slots,
+                         bool emit) {
+    const u32 lane = lane_id();
+    QState& q = qs[t.qi];
+    const u32 n = q.desc->n;
+    if (warp_ld_volatile_u32(&q.stop)) return;
+    u64 count = 0, bytes = 0, calls = 0;
+    u32 iter = 0;
+    if (n == 1) {  // single-vertex query: every root candidate is an embedding
+        count = t.e - t.b;
+        calls = count;
+        if (emit) {
+            for (u32 i = t.b + lane; i < t.e; i += 32) {
+                unsigned long long r = atomicAdd((unsigned long long*)&q.emit_rows, 1ull);
+                if (r < q.emit_cap_rows) q.emit_buf[r] = g.orig[q.list[q.order[0]][i]];
+            }
+        }
+        publish(q, count, bytes, calls);
+        return;
+    }
+    if (t.kind == KIND_EDGES) {
+        // Pairs (root r, depth-1 candidate c) taken from the entries [b, e)
+        // of the first table T[u_0][u_1]; the root of an entry is found by
+        // walking the table's row offsets.
+        const u32 base = q.bn_tab[1][0];
+        const u32* list0 = q.list[q.order[0]];
+        const u32* list1 = q.list[q.order[1]];
+        const bool same01 = q.same_mask[1] & 1u;
+        u32 lo = 0, hi = q.root_cnt;  // largest r with P[base + r] <= b
+        while (hi - lo > 1) {
+            u32 mid = (lo + hi) >> 1;
+            if (q.P[base + mid] <= t.b)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        u32 r = lo;
+        u32 end = t.e;
+        for (u32 e = t.b; e < end; ++e) {
+            while (q.P[base + r + 1] <= e) ++r;
+            const u32 c = q.adj[e];
+            const u32 v0 = list0[r], v1 = list1[c];
+            calls += 1;
+            if (same01 && v0 == v1) continue;
+            __syncwarp();
+            if (lane == 0) {
+                ws->pos[0] = r;
+                ws->vid[0] = v0;
+                ws->pos[1] = c;
+                ws->vid[1] = v1;
+            }
+            __syncwarp();
+            // edge pools are built for queries of four or more vertices
+            setup_level(q, 2, ws, bytes);
+            if (!dfs(g, q, t.qi, 2, ws, ctl, slots, emit, count, bytes, calls, iter)) break;
+            if (e + 2 < end) try_donate_range(ctl, slots, KIND_EDGES, t.qi, 0, e + 1, end, 0, ws, 2u);
+        }
+        publish(q, count, bytes, calls);
+        return;
+    }
+    // Restore the data vertices of the prefix.
+    if (lane < t.d0) ws->vid[lane] = q.list[q.order[lane]][ws->pos[lane]];
+    __syncwarp();
+    const u32 d0 = t.d0;
+    if (t.kind == KIND_FULL && d0 + 1 == n) {
+        // donated entry whose children are the last depth
+        count += emit ? emit_last(q, g, d0, ws, bytes, calls) : count_last(q, d0, ws, bytes, calls);
+    } else {
+        if (t.kind == KIND_FULL) {
+            setup_level(q, d0, ws, bytes);
+        } else {
+            __syncwarp();
+            if (lane == 0) {
+                ws->cur[d0] = t.b;
+                ws->end[d0] = t.e;
+                ws->drv[d0] = t.drv;
+                ws->cn[d0] = 0;
+                ws->ci[d0] = 0;
+            }
+            __syncwarp();
+        }
+        dfs(g, q, t.qi, d0, ws, ctl, slots, emit, count, bytes, calls, iter);
+    }
+    publish(q, count, bytes, calls);
+}
+
+// Initial pool: ticket -> (query, unit range); grab_prefix[i] = grabs of the
+// queries before i.
+__device__ bool take_initial(EnumCtl* ctl, const u32* grab_prefix, const PoolInfo* pools, QState* qs, TaskHdr& t) {
     const u32 lane = lane_id();
     // Once the ticket passes the end it never comes back; skipping the
     // pending increment then keeps idle warps from holding `pending` above
     // zero with transient increments.
-    if (ld_volatile_u32(&ctl->root_ticket) >= ctl->total_roots) return false;
+    if (warp_ld_volatile_u32(&ctl->ticket) >= ctl->total_grabs) return false;
     u32 r = 0, crossing = 0;
     if (lane == 0) {
         atomicAdd(&ctl->pending, 1ull);
         __threadfence();
-        r = atomicAdd(&ctl->root_ticket, grab);
-        if (r >= ctl->total_roots) {
+        r = atomicAdd(&ctl->ticket, 1u);
+        if (r >= ctl->total_grabs) {
             atomicAdd(&ctl->pending, (unsigned long long)-1ll);
-        } else if (r + grab >= ctl->total_roots) {
+        } else if (r + 1 == ctl->total_grabs) {
             crossing = 1;  // this grab exhausts the pool: release the pool's token
         }
     }
     r = __shfl_sync(FULL_MASK, r, 0);
     crossing = __shfl_sync(FULL_MASK, crossing, 0);
-    if (r >= ctl->total_roots) return false;
+    if (r >= ctl->total_grabs) return false;
     if (crossing && lane == 0) {
         __threadfence();
         atomicAdd(&ctl->pending, (unsigned long long)-1ll);
     }
-    // query owning root r
-    u32 lo = 0, hi = ctl->nq;
+    u32 lo = 0, hi = ctl->nq;  // query owning grab r
     while (hi - lo > 1) {
         u32 mid = (lo + hi) >> 1;
-        if (prefix[mid] <= r)
+        if (grab_prefix[mid] <= r)
             lo = mid;
         else
             hi = mid;
     }
+    const PoolInfo& pi = pools[lo];
+    const u32 j = r - grab_prefix[lo];
+    const u32 ub = j * pi.grab, ue = min(pi.units, ub + pi.grab);
+    t.kind = pi.kind;
     t.qi = lo;
     t.d0 = 0;
-    t.b = r - prefix[lo];
-    t.e = min(prefix[lo + 1], r + grab) - prefix[lo];
+    t.b = pi.first + ub;
+    t.e = pi.first + ue;
     t.drv = 0;
     return true;
 }
 
-__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) enum_kernel(DevGraph g, QState* qs, EnumCtl* ctl,
-                                                                    Slot* slots, const u32* prefix, int emit) {
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 4) enum_kernel(DevGraph g, QState* qs, EnumCtl* ctl,
+                                                                    Slot* slots, const u32* grab_prefix,
+                                                                    const PoolInfo* pools, int emit) {
     __shared__ WarpStack stacks[WARPS_PER_BLOCK];
     WarpStack* ws = &stacks[threadIdx.x >> 5];
     const u32 lane = lane_id();
-    Task t;
+    TaskHdr t;
     bool hungry = false;
-    u64 spins = 0;
+    u64 spins = 0, ntasks = 0, npolls = 0;
     while (true) {
-        bool got = take_root(ctl, prefix, qs, t, 1);
-        if (!got) got = dequeue(ctl, slots, t);
+        bool got = take_initial(ctl, grab_prefix, pools, qs, t);
+        if (!got) got = dequeue(ctl, slots, t, ws);
         if (got) {
             if (hungry && lane == 0) atomicSub(&ctl->hungry, 1u);
             hungry = false;
             spins = 0;
             run_task(g, qs, t, ws, ctl, slots, emit != 0);
+            ++ntasks;
             __syncwarp();
             if (lane == 0) {
                 __threadfence();
@@ -619,6 +738,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) enum_kernel(DevGraph g, 
         pend = __shfl_sync(FULL_MASK, pend, 0);
         if (pend == 0) break;
         ++spins;
+        ++npolls;
         if ((spins & 255u) == 0) {
             u32 bail = 0;
             if (lane == 0 && (global_timer_ns() > ctl->deadline_ns + 2000000000ull || spins > (1ull << 32))) {
@@ -627,22 +747,49 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32) enum_kernel(DevGraph g, 
             }
             if (__shfl_sync(FULL_MASK, bail, 0)) break;
         }
-        __nanosleep(200);
+        __nanosleep(256);
+    }
+    if (lane == 0) {
+        atomicAdd((unsigned long long*)&ctl->tasks, (unsigned long long)ntasks);
+        atomicAdd((unsigned long long*)&ctl->idle_polls, (unsigned long long)npolls);
     }
 }
 
-__global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, u32* prefix, u64 budget_ns) {
-    // single block: prefix of root counts, queue sequence numbers
+// Single block: per-query initial pools (edges of the first table for
+// queries of four or more vertices, roots otherwise), their prefix in grabs,
+// and the queue's sequence numbers.
+__global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, u32* grab_prefix, PoolInfo* pools,
+                                 u32 total_warps, u64 budget_ns) {
     __shared__ u32 s_carry;
+    __shared__ u32 wt[32];
     if (threadIdx.x == 0) s_carry = 0;
     __syncthreads();
     for (u32 base = 0; base < nq; base += blockDim.x) {
-        u32 i = base + threadIdx.x;
-        u32 v = 0;
-        if (i < nq) v = (qs[i].status == PSM_DEV_OK && !qs[i].stop) ? qs[i].root_cnt : 0u;
-        // block scan (simple: warp scans + shared totals)
-        __shared__ u32 wt[32];
-        u32 incl = warp_incl_scan(v);
+        const u32 i = base + threadIdx.x;
+        u32 grabs = 0;
+        if (i < nq) {
+            const QState& q = qs[i];
+            PoolInfo pi{KIND_RANGE, 0, 1, 0};
+            if (q.status == PSM_DEV_OK && !q.stop && q.root_cnt > 0) {
+                const u32 n = q.desc->n;
+                if (n >= 4) {
+                    const u32 tb = q.bn_tab[1][0];
+                    pi.kind = KIND_EDGES;
+                    pi.first = q.P[tb];
+                    pi.units = q.P[tb + q.root_cnt] - pi.first;
+                } else {
+                    pi.kind = KIND_RANGE;
+                    pi.first = 0;
+                    pi.units = q.root_cnt;
+                }
+                // about 8 grabs per warp for a lone query; never below one unit
+                const u32 target = total_warps * 8u;
+                pi.grab = max(1u, pi.units / max(1u, target));
+                grabs = (pi.units + pi.grab - 1) / pi.grab;
+            }
+            pools[i] = pi;
+        }
+        u32 incl = warp_incl_scan(grabs);
         if (lane_id() == 31) wt[threadIdx.x >> 5] = incl;
         __syncthreads();
         if (threadIdx.x < 32) {
@@ -651,24 +798,26 @@ __global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, 
             wt[threadIdx.x] = xi - x;
         }
         __syncthreads();
-        u32 excl = s_carry + wt[threadIdx.x >> 5] + incl - v;
-        if (i < nq) prefix[i] = excl;
+        const u32 excl = s_carry + wt[threadIdx.x >> 5] + incl - grabs;
+        if (i < nq) grab_prefix[i] = excl;
         __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) s_carry = excl + v;
+        if (threadIdx.x == blockDim.x - 1) s_carry = excl + grabs;
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        prefix[nq] = s_carry;
-        ctl->total_roots = s_carry;
-        ctl->root_ticket = 0;
+        grab_prefix[nq] = s_carry;
+        ctl->total_grabs = s_carry;
+        ctl->ticket = 0;
         ctl->hungry = 0;
         ctl->q_head = 0;
         ctl->q_tail = 0;
         ctl->error = 0;
         ctl->nq = nq;
-        ctl->pending = s_carry > 0 ? 1ull : 0ull;  // the root pool's token
+        ctl->pending = s_carry > 0 ? 1ull : 0ull;  // the initial pool's token
         ctl->deadline_ns = global_timer_ns() + budget_ns;
         ctl->donations = 0;
+        ctl->tasks = 0;
+        ctl->idle_polls = 0;
     }
     for (u32 i = threadIdx.x; i < QCAP; i += blockDim.x) slots[i].seq = i;
 }
@@ -691,6 +840,8 @@ __global__ void gather_kernel(const QState* qs, u32 nq, DevResult* out) {
     }
 }
 
+size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
 }  // namespace
 
 cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st) {
@@ -699,16 +850,23 @@ cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStre
     return cudaGetLastError();
 }
 
-size_t psm_enum_scratch_bytes() { return sizeof(EnumCtl) + sizeof(Slot) * QCAP + 64; }
+size_t psm_enum_scratch_bytes() { return align16(sizeof(EnumCtl)) + sizeof(Slot) * QCAP + 64; }
 
-cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, u32* prefix, u64 budget_ns,
+// Per-query scratch of the enumeration: grab prefix (nq + 1 words) and pool
+// descriptors.
+size_t psm_enum_query_bytes(u32 nq) { return align16(sizeof(u32) * (nq + 1)) + sizeof(PoolInfo) * nq; }
+
+cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
                             int emit, int blocks, cudaStream_t st) {
     EnumCtl* ctl = (EnumCtl*)scratch;
-    Slot* slots = (Slot*)((char*)scratch + ((sizeof(EnumCtl) + 15) & ~(size_t)15));
-    enum_init_kernel<<<1, 1024, 0, st>>>(qs, nq, ctl, slots, prefix, budget_ns);
+    Slot* slots = (Slot*)((char*)scratch + align16(sizeof(EnumCtl)));
+    u32* grab_prefix = (u32*)query_scratch;
+    PoolInfo* pools = (PoolInfo*)((char*)query_scratch + align16(sizeof(u32) * (nq + 1)));
+    enum_init_kernel<<<1, 1024, 0, st>>>(qs, nq, ctl, slots, grab_prefix, pools,
+                                         (u32)blocks * WARPS_PER_BLOCK, budget_ns);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    enum_kernel<<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, prefix, emit);
+    enum_kernel<<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, grab_prefix, pools, emit);
     return cudaGetLastError();
 }
 
@@ -724,14 +882,16 @@ cudaError_t psm_enum_max_blocks(int* blocks) {
     return cudaSuccess;
 }
 
-// Reads back the launch-wide error flag and donation count.
-cudaError_t psm_enum_read_ctl(void* scratch, u32* error, u64* donations, cudaStream_t st) {
+// Reads back the launch-wide error flag and scheduling counters.
+cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st) {
     EnumCtl h;
     cudaError_t e = cudaMemcpyAsync(&h, scratch, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) return e;
     e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return e;
-    *error = h.error;
-    *donations = h.donations;
+    out->error = h.error;
+    out->donations = h.donations;
+    out->tasks = h.tasks;
+    out->idle_polls = h.idle_polls;
     return cudaSuccess;
 }

@@ -38,8 +38,9 @@ cudaError_t psm_launch_prep_grid(const DevGraph& g, QState* qs, void* barrier, D
                                  int blocks, int threads, cudaStream_t st);
 cudaError_t psm_prep_grid_max_blocks(int threads, int* blocks);
 size_t psm_enum_scratch_bytes();
-cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, u32* prefix, u64 budget_ns,
+size_t psm_enum_query_bytes(u32 nq);
+cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
                             int emit, int blocks, cudaStream_t st);
 cudaError_t psm_enum_max_blocks(int* blocks);
 cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st);
-cudaError_t psm_enum_read_ctl(void* scratch, u32* error, u64* donations, cudaStream_t st);
+cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st);

@@ -761,7 +761,7 @@ __device__ void cfl_order_select(QState& q, const u32* pw) {
 // Backward neighbours by depth (matching/EvaluateQuery.cpp:1594-1625: all
 // earlier neighbours, in query-vertex id order), their table rows, and the
 // earlier depths sharing the label (only those can collide on a data vertex).
-__device__ void enum_plan(QState& q) {
+__device__ void enum_plan(const DevGraph& g, QState& q) {
     const QDesc* d = q.desc;
     const u32 n = d->n;
     u32 depth_of[PSM_MAXQ];
@@ -784,6 +784,7 @@ __device__ void enum_plan(QState& q) {
         q.same_mask[i] = same;
         seen |= 1u << u;
     }
+    for (u32 u = 0; u < n; ++u) q.cbase[u] = bucket_base(g, d->label[u]);
     q.root_cnt = q.cnt[q.order[0]];
     u64 mem = 0;
     for (u32 u = 0; u < n; ++u) mem += (u64)q.cnt[u] * 4u;
@@ -922,7 +923,7 @@ __device__ void prepare_query(Team& t, const DevGraph& g, QState& q, DevArena* a
     }
     TSYNC(t);
     if (t.rank() == 0) {
-        enum_plan(q);
+        enum_plan(g, q);
         if (q.empty) q.root_cnt = 0;
     }
     TSYNC(t);

@@ -131,6 +131,7 @@ struct QState {
     u32 bn_depth[PSM_MAXQ][PSM_MAXQ - 1];
     u32 bn_tab[PSM_MAXQ][PSM_MAXQ - 1];   // row base into P for table T[bn][u_d]
     u32 same_mask[PSM_MAXQ];              // earlier depths with the same label
+    u32 cbase[PSM_MAXQ];                  // first internal id of the bucket of u (by query vertex)
     u32 root_cnt;
     // results
     u64 count;
@@ -149,6 +150,12 @@ struct QState {
 struct DevResult {
     u64 count, calls, alg_bytes, memory_bytes, table_nnz, emit_rows;
     u32 status, overtime, filter_ok, empty;
+};
+
+// Launch-wide counters of the enumeration scheduler, read back by the host.
+struct EnumStats {
+    u32 error;
+    u64 donations, tasks, idle_polls;
 };
 
 // Device-side bump allocator over an arena region.
