@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -69,6 +70,7 @@ struct psm_context {
     int prep_threads = 512;
     int prep_grid_blocks = 0;
     int prep_block_blocks = 0;
+    int cluster_size = 0;  // > 0: plain-path preparation by one thread-block cluster of this size
     int enum_blocks = 0;
     cudaEvent_t ev[4]{};
     std::vector<char> host_stage;  // QDesc / QState staging
@@ -115,16 +117,27 @@ int setup_query(psm_context* ctx, const psm_graph& g, const QDesc& d, const psm_
     if (rows >= 0xFFFFFFF0ull) return fail(PSM_ERR_ARG, "candidate tables too large for 32-bit offsets");
     q.acc = b.take<u32>(maxw);
     q.tmp = b.take<u32>(maxw);
+    q.acc_words = maxw;
     q.P = b.take<u32>(rows + 1);
     q.scan = b.take<u32>(scan_words);
     if (d.order == PSM_ORDER_CFL) {
-        q.est_a = b.take<u64>(maxb);
-        q.est_b = b.take<u64>(maxb);
+        // one buffer pair per block that estimates paths concurrently
+        q.est_blocks = std::max(1u, std::min(64u, scan_words - 1));
+        q.est_stride = maxb;
+        q.est_a = b.take<u64>((size_t)q.est_blocks * 2 * maxb);
         q.est_out = b.take<u64>(PSM_PLAN_WORDS);
-        if (!q.est_a || !q.est_b || !q.est_out) return fail(PSM_ERR_OOM, "device arena exhausted (estimates)");
+        if (!q.est_a || !q.est_out) return fail(PSM_ERR_OOM, "device arena exhausted (estimates)");
     }
     if (!q.acc || !q.tmp || !q.P || !q.scan) return fail(PSM_ERR_OOM, "device arena exhausted (tables)");
     q.cap = opt.cap;
+    // Diagnostics: PSM_TRACE=1 records a device timestamp per preparation
+    // step (printed to stderr); PSM_HYBRID=1 lets block 0 of the plain-path
+    // grid run small steps alone.
+    if (getenv("PSM_TRACE")) {
+        q.trace = b.take<u64>(PSM_TRACE_STEPS + 1);
+        if (!q.trace) return fail(PSM_ERR_OOM, "device arena exhausted (trace)");
+    }
+    if (getenv("PSM_HYBRID")) q.step_cursor = HYBRID_REQUEST;
     if (opt.emit) {
         q.emit_cap_rows = opt.emit_capacity;
         q.emit_buf = b.take<u32>((size_t)opt.emit_capacity * d.n);
@@ -175,7 +188,8 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     lay.d_enum_q = b.take<char>(psm_enum_query_bytes(nq));
     lay.d_res = b.take<DevResult>(nq);
     if (!lay.d_desc || !lay.d_q || !lay.d_enum_q || !lay.d_res) return fail(PSM_ERR_OOM, "device arena exhausted");
-    const u32 scan_words = grid_team ? (u32)ctx->prep_grid_blocks + 1 : 2u;
+    // team scans need one word per block of the preparing team (+1)
+    const u32 scan_words = grid_team ? (u32)std::max(ctx->prep_grid_blocks, ctx->cluster_size) + 1 : 2u;
     std::vector<QState> hq(nq);
     for (u32 i = 0; i < nq; ++i) {
         int rc = setup_query(ctx, *g, descs[i], opt, b, lay.d_desc + i, scan_words, hq[i]);
@@ -197,7 +211,9 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     CK(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), ctx->st));
     const u64 budget = budget_ns(opt);
     CK(cudaEventRecord(ctx->ev[0], ctx->st));
-    if (grid_team) {
+    if (grid_team && ctx->cluster_size > 0) {
+        CK(psm_launch_prep_cluster(g->dev, lay.d_q, ctx->d_devarena, ctx->cluster_size, ctx->prep_threads, ctx->st));
+    } else if (grid_team) {
         CK(psm_launch_prep_grid(g->dev, lay.d_q, ctx->d_barrier, ctx->d_devarena, budget, ctx->prep_grid_blocks,
                                 ctx->prep_threads, ctx->st));
     } else {
@@ -232,10 +248,24 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     }
     if (grid_team) {
         u32 ab = 0;
-        CK(cudaMemcpy(&ab, (char*)ctx->d_barrier + 8, sizeof(u32), cudaMemcpyDeviceToHost));
+        // GridBarrier::abort (second word of the barrier)
+        CK(cudaMemcpy(&ab, (char*)ctx->d_barrier + 4, sizeof(u32), cudaMemcpyDeviceToHost));
         if (ab) {
             for (u32 i = 0; i < nq; ++i) results[i].status = PSM_ERR_INTERNAL;
             worst = PSM_ERR_INTERNAL;
+        }
+    }
+    if (hq[0].trace) {
+        for (u32 i = 0; i < nq && i < 4; ++i) {
+            std::vector<u64> tr(PSM_TRACE_STEPS + 1);
+            CK(cudaMemcpy(tr.data(), hq[i].trace, tr.size() * sizeof(u64), cudaMemcpyDeviceToHost));
+            fprintf(stderr, "psm trace q%u:", i);
+            u64 prev = tr[PSM_TRACE_STEPS];
+            for (u32 k = 0; k < PSM_TRACE_STEPS && tr[k] >= prev && tr[k] - prev < 10000000000ull; ++k) {
+                fprintf(stderr, " %u:%.1f", k, (tr[k] - prev) / 1e3);
+                prev = tr[k];
+            }
+            fprintf(stderr, " (us)\n");
         }
     }
     if (keep) {
@@ -333,6 +363,15 @@ int psm_context_create(int device, uint64_t arena_bytes, psm_context** out) {
         return fail(PSM_ERR_CUDA, "occupancy query failed");
     }
     c->prep_block_blocks = prop.multiProcessorCount * 4;
+    // Plain-path preparation team: the whole grid (default; measured fastest
+    // on B200) or one thread-block cluster (PSM_PLAIN_TEAM=cluster,
+    // PSM_CLUSTER=size).
+    const char* team = getenv("PSM_PLAIN_TEAM");
+    if (team && strcmp(team, "cluster") == 0) {
+        int want = 16;
+        if (const char* cs = getenv("PSM_CLUSTER")) want = std::max(1, std::min(16, atoi(cs)));
+        if (psm_prep_cluster_size(c->prep_threads, want, &c->cluster_size) != cudaSuccess) c->cluster_size = 0;
+    }
     *out = c;
     return PSM_OK;
 }

@@ -37,6 +37,9 @@ cudaError_t psm_launch_prep_block(const DevGraph& g, QState* qs, u32 nq, u32* ti
 cudaError_t psm_launch_prep_grid(const DevGraph& g, QState* qs, void* barrier, DevArena* arena, u64 budget_ns,
                                  int blocks, int threads, cudaStream_t st);
 cudaError_t psm_prep_grid_max_blocks(int threads, int* blocks);
+cudaError_t psm_prep_cluster_size(int threads, int want, int* size);
+cudaError_t psm_launch_prep_cluster(const DevGraph& g, QState* qs, DevArena* arena, int cluster, int threads,
+                                    cudaStream_t st);
 size_t psm_enum_scratch_bytes();
 size_t psm_enum_query_bytes(u32 nq);
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,

@@ -372,7 +372,10 @@ int psm_build_qdesc(const psm_graph& g, const psm_query_desc& qd, const psm_opti
     u32 e = 0;
     for (u32 x = 0; x < n; ++x) {
         d->e_first[x] = e;
-        for (u32 y : q.nbrs[x]) d->e_dst[e++] = y;
+        for (u32 y : q.nbrs[x]) {
+            d->e_src[e] = x;
+            d->e_dst[e++] = y;
+        }
     }
     d->e_first[n] = e;
     return PSM_OK;

@@ -13,10 +13,13 @@
 // (GQL refinement of u = 0..q-1, the CFL generate / prune steps) are
 // separated by team barriers and keep that order, which makes the candidate
 // sets identical to the reference's.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "device_util.cuh"
 #include "psm_internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace {
 
@@ -36,15 +39,16 @@ struct BlockTeam {
 };
 
 struct GridBarrier {
-    u32 count;
-    u32 gen;
+    u32 count;  // arrivals; its top bit flips once per completed barrier
     u32 abort;
-    u32 pad;
+    u32 pad[2];
 };
 
-// Whole-grid team for a cooperative launch (all blocks co-resident). The
-// barrier spins with a bounded wait: past the deadline or the iteration cap
-// it raises `abort`, every later barrier returns false at once and the
+// Whole-grid team for a cooperative launch (all blocks co-resident). One
+// release-add per block per barrier: block 0 adds 2^31 - (blocks - 1), the
+// others add 1, so the top bit of `count` flips exactly when every block
+// has arrived. Waits are bounded: past the deadline or the iteration cap a
+// block raises `abort`, every later barrier returns false at once and the
 // kernel unwinds; the host reports an internal error.
 struct GridTeam {
     GridBarrier* bar;
@@ -61,35 +65,46 @@ struct GridTeam {
         if (threadIdx.x == 0) {
             u32 ab = ld_acquire_u32(&bar->abort);
             if (!ab) {
-                __threadfence();
-                u32 g = ld_acquire_u32(&bar->gen);
-                u32 arrived = atomicAdd(&bar->count, 1u);
-                if (arrived == gridDim.x - 1) {
-                    atomicExch(&bar->count, 0u);
-                    __threadfence();
-                    atomicAdd(&bar->gen, 1u);
-                } else {
-                    u32 it = 0;
-                    while (ld_acquire_u32(&bar->gen) == g) {
+                const u32 add = blockIdx.x == 0 ? (0x80000000u - (gridDim.x - 1)) : 1u;
+                u32 old;
+                asm volatile("atom.add.release.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(&bar->count), "r"(add)
+                             : "memory");
+                u32 it = 0;
+                while (((ld_acquire_u32(&bar->count) ^ old) & 0x80000000u) == 0) {
+                    ++it;
+                    if ((it & 63u) == 0) {
                         if (ld_acquire_u32(&bar->abort)) break;
-                        if ((++it & 1023u) == 0 && global_timer_ns() > deadline_ns) {
+                        if ((it & 4095u) == 0 && (global_timer_ns() > deadline_ns || it > (1u << 30))) {
                             atomicExch(&bar->abort, 1u);
                             break;
                         }
-                        if (it > (1u << 30)) {
-                            atomicExch(&bar->abort, 1u);
-                            break;
-                        }
-                        __nanosleep(64);
                     }
+                    if (it > 128) __nanosleep(32);
                 }
-                __threadfence();
                 ab = ld_acquire_u32(&bar->abort);
             }
             s_abort = ab;
         }
         __syncthreads();
         return s_abort == 0;
+    }
+};
+
+// Thread-block cluster team: the blocks of one cluster (co-scheduled on one
+// GPC) share a hardware barrier, so a step costs far less than a grid-wide
+// software barrier. Release/acquire at cluster scope makes the global-memory
+// writes of every block visible to the others after sync().
+struct ClusterTeam {
+    __device__ u32 rank() const { return cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
+    __device__ u32 size() const { return cg::this_cluster().num_blocks() * blockDim.x; }
+    __device__ u32 warp() const { return rank() >> 5; }
+    __device__ u32 nwarps() const { return size() >> 5; }
+    __device__ u32 block() const { return cg::this_cluster().block_rank(); }
+    __device__ u32 nblocks() const { return cg::this_cluster().num_blocks(); }
+    __device__ bool sync() {
+        __threadfence();
+        cg::this_cluster().sync();
+        return true;
     }
 };
 
@@ -342,13 +357,79 @@ __device__ bool mark_neighbours(Team& t, const DevGraph& g, QState& q, u32 p, u3
     return true;
 }
 
+// Contiguous word range of block b in a team scan over N words (the same
+// partition team_scan uses).
+__device__ __forceinline__ u32 scan_block_words(u32 N, u32 nb) { return ((N + nb - 1) / nb + 31u) & ~31u; }
+
+// Second half of a team scan whose per-block totals are already in
+// scratch[0, nblocks): each warp recounts its own words, then emits rank and
+// list entries of bitmap u. *total (by team rank 0) = candidate count.
+template <class Team>
+__device__ bool compact_from_totals(Team& t, const DevGraph& g, QState& q, u32 u) {
+    __shared__ u32 s_wt[32];
+    __shared__ u32 s_bp;
+    const u32 N = q.bwords[u];
+    const u32* bm = q.bm[u];
+    u32* rank = q.rank[u];
+    u32* list = q.list[u];
+    const u32 base = bucket_base(g, q.desc->label[u]);
+    const u32 nb = t.nblocks(), b = t.block();
+    const u32 lane = lane_id(), w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const u32 per_blk = scan_block_words(N, nb);
+    const u32 b0 = min(N, b * per_blk), b1 = min(N, b0 + per_blk);
+    const u32 per_w = ((b1 - b0 + wpb - 1) / wpb + 31u) & ~31u;
+    const u32 w0 = min(b1, b0 + w * per_w), w1 = min(b1, w0 + per_w);
+    u32 s = 0;
+    for (u32 i = w0 + lane; i < w1; i += 32) s += __popc(bm[i]);
+    s = warp_sum(s);
+    if (lane == 0) s_wt[w] = s;
+    if (w == 0) {
+        u32 x = 0, all = 0;
+        for (u32 i = lane; i < nb; i += 32) {
+            u32 v = ld_volatile_u32(q.scan + i);
+            if (i < b) x += v;
+            all += v;
+        }
+        x = warp_sum(x);
+        all = warp_sum(all);
+        if (lane == 0) {
+            s_bp = x;
+            if (b == 0) q.cnt[u] = all;
+        }
+    }
+    __syncthreads();
+    u32 carry = s_bp;
+    for (u32 i = 0; i < w; ++i) carry += s_wt[i];
+    for (u32 base_i = w0; base_i < w1; base_i += 32) {
+        u32 i = base_i + lane;
+        u32 x = i < w1 ? bm[i] : 0u;
+        u32 v = __popc(x);
+        u32 incl = warp_incl_scan(v);
+        if (i < w1) {
+            u32 j = carry + incl - v;
+            rank[i] = j;
+            while (x) {
+                u32 bit = __ffs(x) - 1;
+                x &= x - 1;
+                list[j++] = base + 32u * i + bit;
+            }
+        }
+        carry += __shfl_sync(FULL_MASK, incl, 31);
+    }
+    __syncthreads();
+    return true;
+}
+
+// matching/FilterVertices.cpp:841-912 (generateCandidates): candidates of u
+// are the data vertices of u's label, with enough degree and NLF, adjacent to
+// a live candidate of every pivot. The accumulator bitmaps (acc, tmp) are
+// all-zero between steps: they are cleared once at the start of the query
+// and re-zeroed where they are consumed.
 template <class Team>
 __device__ bool step_generate(Team& t, const DevGraph& g, QState& q, u32 u, u32 pivots) {
     const QDesc* d = q.desc;
     const u32 lu = d->label[u];
     const u32 W = q.bwords[u];
-    for (u32 i = t.rank(); i < W; i += t.size()) q.acc[i] = 0;
-    TSYNC_B(t);
     bool first = true;
     u32 pm = pivots;
     while (pm) {
@@ -356,27 +437,36 @@ __device__ bool step_generate(Team& t, const DevGraph& g, QState& q, u32 u, u32 
         pm &= pm - 1;
         if (first) {
             mark_neighbours(t, g, q, p, lu, q.acc);
-            TSYNC_B(t);
         } else {
-            for (u32 i = t.rank(); i < W; i += t.size()) q.tmp[i] = 0;
-            TSYNC_B(t);
             mark_neighbours(t, g, q, p, lu, q.tmp);
             TSYNC_B(t);
-            for (u32 i = t.rank(); i < W; i += t.size()) q.acc[i] &= q.tmp[i];
-            TSYNC_B(t);
+            for (u32 i = t.rank(); i < W; i += t.size()) {
+                q.acc[i] &= q.tmp[i];
+                q.tmp[i] = 0;
+            }
         }
         first = false;
+        if (!pm)  // the scan's per-block totals start from zero
+            for (u32 i = t.rank(); i < t.nblocks(); i += t.size()) q.scan[i] = 0;
+        TSYNC_B(t);
     }
+    // Survivors: degree + NLF per surviving bit (warp per word); the word's
+    // popcount goes straight to the total of the block that will emit it.
     const u32 lane = lane_id();
     const u32 base = bucket_base(g, lu), bsz = bucket_size(g, lu);
+    const u32 per_blk = scan_block_words(W, t.nblocks());
     for (u32 w = t.warp(); w < W; w += t.nwarps()) {
         u32 pos = 32u * w + lane;
         bool ok = pos < bsz && ((q.acc[w] >> lane) & 1u) && nlf_ok(g, d, u, base + pos);
         u32 word = __ballot_sync(FULL_MASK, ok);
-        if (lane == 0) q.bm[u][w] = word;
+        if (lane == 0) {
+            q.bm[u][w] = word;
+            q.acc[w] = 0;
+            if (word) atomicAdd(q.scan + w / per_blk, (u32)__popc(word));
+        }
     }
     TSYNC_B(t);
-    if (!compact_vertex(t, g, q, u)) return false;
+    if (!compact_from_totals(t, g, q, u)) return false;
     TSYNC_B(t);
     return true;
 }
@@ -443,11 +533,7 @@ __device__ __forceinline__ void row_of(const QState& q, u32 ne, u32 r, u32& e, u
     i = r - q.e_row_base[lo];
 }
 
-__device__ __forceinline__ u32 edge_src(const QDesc* d, u32 e) {
-    u32 x = 0;
-    while (d->e_first[x + 1] <= e) ++x;
-    return x;
-}
+__device__ __forceinline__ u32 edge_src(const QDesc* d, u32 e) { return d->e_src[e]; }
 
 // matching/BuildTable.cpp:9-151: row i of T[x][y] lists, ascending, the
 // positions in C(y) of the data neighbours of C(x)[i]. Every directed query
@@ -457,14 +543,20 @@ template <class Team>
 __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* arena) {
     const QDesc* d = q.desc;
     const u32 ne = d->e_first[d->n];
-    if (t.rank() == 0) {
-        u32 acc = 0;
-        for (u32 e = 0; e < ne; ++e) {
-            q.e_row_base[e] = acc;
-            acc += q.cnt[edge_src(d, e)];
+    if (t.warp() == 0) {  // row bases of the directed edges: warp prefix sum
+        const u32 lane = lane_id();
+        u32 carry = 0;
+        for (u32 e0 = 0; e0 < ne; e0 += 32) {
+            const u32 e = e0 + lane;
+            const u32 v = e < ne ? q.cnt[edge_src(d, e)] : 0u;
+            const u32 incl = warp_incl_scan(v);
+            if (e < ne) q.e_row_base[e] = carry + incl - v;
+            carry += __shfl_sync(FULL_MASK, incl, 31);
         }
-        q.e_row_base[ne] = acc;
-        q.total_rows = acc;
+        if (lane == 0) {
+            q.e_row_base[ne] = carry;
+            q.total_rows = carry;
+        }
     }
     TSYNC_B(t);
     const u32 R = q.total_rows;
@@ -585,58 +677,66 @@ __device__ void gql_order(const DevGraph& g, QState& q) {
             }
 }
 
-// matching/GenerateQueryPlan.cpp:680-721 estimatePathEmbeddsingsNum for all
-// paths of the chosen CFL order plan; est_out[path_off[p] - p + k] is entry k
-// of path p (paths have path_len - 1 estimates).
+// matching/GenerateQueryPlan.cpp:680-721 estimatePathEmbeddsingsNum for one
+// path, by one thread block: est[k-2] = entries of the last table; walking
+// back, a row's estimate is the sum of the estimates of its entries.
+__device__ void estimate_path_block(QState& q, const u32* path, u32 k, u64* est, u64* child, u64* par) {
+    {
+        const u32 a = path[k - 2], b = path[k - 1];
+        const u32 rb = table_base(q, a, b), rows = q.cnt[a];
+        u64 s = 0;
+        for (u32 i = threadIdx.x; i < rows; i += blockDim.x) {
+            u64 c = q.P[rb + i + 1] - q.P[rb + i];
+            child[i] = c;
+            s += c;
+        }
+        s = warp_sum64(s);
+        if (lane_id() == 0 && s) atomicAdd((unsigned long long*)&est[k - 2], (unsigned long long)s);
+    }
+    __syncthreads();
+    for (int i = (int)k - 2; i >= 1; --i) {
+        const u32 a = path[i - 1], b = path[i];
+        const u32 rb = table_base(q, a, b), rows = q.cnt[a];
+        u64 s = 0;
+        for (u32 j = threadIdx.x; j < rows; j += blockDim.x) {
+            u64 ls = 0;
+            for (u32 e = q.P[rb + j]; e < q.P[rb + j + 1]; ++e) ls += child[q.adj[e]];
+            par[j] = ls;
+            s += ls;
+        }
+        s = warp_sum64(s);
+        if (lane_id() == 0 && s) atomicAdd((unsigned long long*)&est[i - 1], (unsigned long long)s);
+        __syncthreads();
+        u64* tmp = child;
+        child = par;
+        par = tmp;
+    }
+}
+
+// Estimates of all paths of the chosen CFL order plan; entry k of path p is
+// est_out[path_off[p] - p + k] (a path of length l has l - 1 estimates).
+// Paths are independent: with several blocks each block takes its own paths
+// (its own child / parent buffers), so the whole step costs one team barrier.
 template <class Team>
 __device__ bool cfl_estimates(Team& t, QState& q, const u32* pw) {
     const QDesc* d = q.desc;
     const u32 n = d->n;
-    const u32 ngroups = pw[1 + 2 * n + 1];
-    const u32* gfirst = pw + 1 + 2 * n + 2;
-    const u32 npaths = gfirst[ngroups + 1 - 1 + 1];
+    const u32 ncore = pw[1 + 2 * n];
+    const u32 ngroups = pw[2 + 2 * n];
+    const u32* gfirst = pw + 3 + 2 * n;
+    const u32 npaths = gfirst[ngroups + 1];
     const u32* poff = gfirst + ngroups + 2;
-    const u32* ncore_p = pw + 1 + 2 * n;
-    const u32* pv = poff + npaths + 1 + ncore_p[0];
+    const u32* pv = poff + npaths + 1 + ncore;
     for (u32 i = t.rank(); i < PSM_PLAN_WORDS; i += t.size()) q.est_out[i] = 0;
     TSYNC_B(t);
-    for (u32 p = 0; p < npaths; ++p) {
-        const u32* path = pv + poff[p];
-        const u32 k = poff[p + 1] - poff[p];
-        u64* est = q.est_out + (poff[p] - p);
-        u64* child = q.est_a;
-        u64* par = q.est_b;
-        {
-            const u32 a = path[k - 2], b = path[k - 1];
-            const u32 rb = table_base(q, a, b), rows = q.cnt[a];
-            u64 s = 0;
-            for (u32 i = t.rank(); i < rows; i += t.size()) {
-                u64 c = q.P[rb + i + 1] - q.P[rb + i];
-                child[i] = c;
-                s += c;
-            }
-            s = warp_sum64(s);
-            if (lane_id() == 0 && s) atomicAdd((unsigned long long*)&est[k - 2], (unsigned long long)s);
-        }
-        TSYNC_B(t);
-        for (int i = (int)k - 2; i >= 1; --i) {
-            const u32 a = path[i - 1], b = path[i];
-            const u32 rb = table_base(q, a, b), rows = q.cnt[a];
-            u64 s = 0;
-            for (u32 j = t.rank(); j < rows; j += t.size()) {
-                u64 ls = 0;
-                for (u32 e = q.P[rb + j]; e < q.P[rb + j + 1]; ++e) ls += child[q.adj[e]];
-                par[j] = ls;
-                s += ls;
-            }
-            s = warp_sum64(s);
-            if (lane_id() == 0 && s) atomicAdd((unsigned long long*)&est[i - 1], (unsigned long long)s);
-            TSYNC_B(t);
-            u64* tmp = child;
-            child = par;
-            par = tmp;
-        }
+    const u32 eb = min(t.nblocks(), q.est_blocks);
+    if (t.block() < eb) {
+        u64* child = q.est_a + (size_t)t.block() * 2 * q.est_stride;
+        u64* par = child + q.est_stride;
+        for (u32 p = t.block(); p < npaths; p += eb)
+            estimate_path_block(q, pv + poff[p], poff[p + 1] - poff[p], q.est_out + (poff[p] - p), child, par);
     }
+    TSYNC_B(t);
     return true;
 }
 
@@ -759,126 +859,186 @@ __device__ void cfl_order_select(QState& q, const u32* pw) {
 }
 
 // Backward neighbours by depth (matching/EvaluateQuery.cpp:1594-1625: all
-// earlier neighbours, in query-vertex id order), their table rows, and the
-// earlier depths sharing the label (only those can collide on a data vertex).
-__device__ void enum_plan(const DevGraph& g, QState& q) {
+// earlier neighbours, in query-vertex id order), their table rows, the
+// earlier depths sharing the label (only those can collide on a data
+// vertex), and computeMemoryCostInBytes (BuildTable.cpp:300-326). One warp:
+// lane i handles depth i; all loops are warp-uniform.
+__device__ void enum_plan_warp(const DevGraph& g, QState& q) {
     const QDesc* d = q.desc;
     const u32 n = d->n;
-    u32 depth_of[PSM_MAXQ];
-    for (u32 i = 0; i < n; ++i) depth_of[q.order[i]] = i;
-    u32 seen = 0;
-    for (u32 i = 0; i < n; ++i) {
-        const u32 u = q.order[i];
-        u32 k = 0, same = 0;
-        u32 m = d->adj[u] & seen;
-        while (m) {
-            u32 b = __ffs(m) - 1;
-            m &= m - 1;
-            q.bn_depth[i][k] = depth_of[b];
-            q.bn_tab[i][k] = table_base(q, b, u);
+    const u32 lane = lane_id();
+    const bool act = lane < n;
+    const u32 u = act ? q.order[lane] : 0u;          // vertex at depth lane
+    const u32 lab = act ? d->label[u] : 0xFFFFFFFFu;  // its label
+    u32 depth_of = 0;                                 // depth of vertex `lane`
+    for (u32 j = 0; j < n; ++j)
+        if (__shfl_sync(FULL_MASK, u, j) == lane) depth_of = j;
+    u32 seen_incl = act ? (1u << u) : 0u;  // vertices at depths <= lane
+    for (u32 o = 1; o < 32; o <<= 1) {
+        u32 y = __shfl_up_sync(FULL_MASK, seen_incl, o);
+        if (lane >= o) seen_incl |= y;
+    }
+    const u32 seen = seen_incl & ~(act ? (1u << u) : 0u);
+    const u32 m = act ? (d->adj[u] & seen) : 0u;
+    u32 k = 0, same = 0;
+    for (u32 b = 0; b < n; ++b) {
+        const u32 db = __shfl_sync(FULL_MASK, depth_of, b);
+        if ((m >> b) & 1u) {
+            q.bn_depth[lane][k] = db;
+            q.bn_tab[lane][k] = table_base(q, b, u);
             ++k;
         }
-        for (u32 j = 0; j < i; ++j)
-            if (d->label[q.order[j]] == d->label[u]) same |= 1u << j;
-        q.nbn[i] = k;
-        q.same_mask[i] = same;
-        seen |= 1u << u;
+        const u32 lb = __shfl_sync(FULL_MASK, lab, b);
+        if (b < lane && lb == lab) same |= 1u << b;
     }
-    for (u32 u = 0; u < n; ++u) q.cbase[u] = bucket_base(g, d->label[u]);
-    q.root_cnt = q.cnt[q.order[0]];
+    if (act) {
+        q.nbn[lane] = k;
+        q.same_mask[lane] = same;
+        q.cbase[lane] = bucket_base(g, d->label[lane]);
+    }
+    // memory cost: candidates of every vertex, both tables of every edge
     u64 mem = 0;
-    for (u32 u = 0; u < n; ++u) mem += (u64)q.cnt[u] * 4u;
-    for (u32 a = 0; a < n; ++a) {
-        u32 m = d->adj[a] & ~((2u << a) - 1u);  // b > a
-        while (m) {
-            u32 b = __ffs(m) - 1;
-            m &= m - 1;
-            u32 ab = table_base(q, a, b), ba = table_base(q, b, a);
-            u64 nab = q.P[ab + q.cnt[a]] - q.P[ab], nba = q.P[ba + q.cnt[b]] - q.P[ba];
+    if (act) {
+        const u32 a = lane;
+        mem += (u64)q.cnt[a] * 4u;
+        u32 mb = d->adj[a] & ~((2u << a) - 1u);  // neighbours b > a
+        while (mb) {
+            const u32 b = __ffs(mb) - 1;
+            mb &= mb - 1;
+            const u32 ab = table_base(q, a, b), ba = table_base(q, b, a);
+            const u64 nab = q.P[ab + q.cnt[a]] - q.P[ab], nba = q.P[ba + q.cnt[b]] - q.P[ba];
             mem += (nab + q.cnt[a] + nba + q.cnt[b]) * 4u;
         }
     }
-    q.memory_bytes = mem;
+    mem = warp_sum64(mem);
+    if (lane == 0) {
+        q.memory_bytes = mem;
+        q.root_cnt = q.empty ? 0u : q.cnt[q.order[0]];
+    }
 }
 
 // ------------------------------------------------------------ driver --
 
-template <class Team>
-__device__ void prepare_query(Team& t, const DevGraph& g, QState& q, DevArena* arena) {
+// ------------------------------------------------------------ driver --
+//
+// The preparation of a query is a fixed list of steps, each ending with a
+// team barrier:
+//   0 clear, 1 NLF, 2 pick start vertices,
+//   GQL / NLF filter: compact every u, empty check, [GQL: refine (round, u)
+//     for 2n steps, compact every u],
+//   CFL filter: compact the start vertex, the plan's generate / prune steps,
+//   then: empty check, tables, order, enumeration plan.
+// run_step executes one step with any team; the drivers below choose teams.
+
+__device__ __forceinline__ bool is_cfl(const QDesc* d) { return d->filter == PSM_FILTER_CFL; }
+
+// Number of steps (valid once step 2 has picked the CFL start vertex).
+__device__ u32 step_count(const QState& q) {
     const QDesc* d = q.desc;
     const u32 n = d->n;
-    // Stage 0: clear bitmaps and counters.
-    for (u32 u = 0; u < n; ++u)
-        for (u32 i = t.rank(); i < q.bwords[u]; i += t.size()) q.bm[u][i] = 0;
-    if (t.rank() == 0) {
-        for (u32 i = 0; i < PSM_MAXQ + PSM_MAXOPT; ++i) q.item_cnt[i] = 0;
-        q.empty = 0;
-        q.filter_ok = 1;
-        q.count = 0;
-        q.calls = 0;
-        q.alg_bytes = 0;
-        q.stop = 0;
-        q.overtime = 0;
-        q.emit_rows = 0;
-        q.table_nnz = 0;
-        q.memory_bytes = 0;
-        q.status = PSM_DEV_OK;
+    u32 mid;
+    if (is_cfl(d))
+        mid = 1 + d->fplan[q.froot].nsteps;
+    else
+        mid = n + 1 + (d->filter == PSM_FILTER_GQL ? 3 * n : 0);
+    return 3 + mid + 4;
+}
+
+template <class Team>
+__device__ bool run_step(Team& t, const DevGraph& g, QState& q, DevArena* arena, u32 k) {
+    const QDesc* d = q.desc;
+    const u32 n = d->n;
+    const bool cfl = is_cfl(d);
+    if (k == 0) {  // clear bitmaps and counters
+        for (u32 u = 0; u < n; ++u)
+            for (u32 i = t.rank(); i < q.bwords[u]; i += t.size()) q.bm[u][i] = 0;
+        if (cfl)
+            for (u32 i = t.rank(); i < q.acc_words; i += t.size()) {
+                q.acc[i] = 0;
+                q.tmp[i] = 0;
+            }
+        if (t.rank() == 0) {
+            for (u32 i = 0; i < PSM_MAXQ + PSM_MAXOPT; ++i) q.item_cnt[i] = 0;
+            q.empty = 0;
+            q.filter_ok = 1;
+            q.count = 0;
+            q.calls = 0;
+            q.alg_bytes = 0;
+            q.stop = 0;
+            q.overtime = 0;
+            q.emit_rows = 0;
+            q.table_nnz = 0;
+            q.memory_bytes = 0;
+            q.root_cnt = 0;
+            q.status = PSM_DEV_OK;
+        }
+        TSYNC_B(t);
+        return true;
     }
-    TSYNC(t);
-    const u32 all = n >= 32 ? ~0u : ((1u << n) - 1u);
-    const bool cfl = d->filter == PSM_FILTER_CFL;
-    u32 need = all;
-    if (cfl) {
-        need = 0;
-        for (u32 k = 0; k < d->nfopt; ++k) need |= 1u << d->fopt_vertex[k];
-    }
-    stage_nlf(t, g, q, need, d->order == PSM_ORDER_CFL);
-    TSYNC(t);
-    if (t.rank() == 0) {
+    if (k == 1) {  // NLF candidates of the needed items
+        u32 need = n >= 32 ? ~0u : ((1u << n) - 1u);
         if (cfl) {
+            need = 0;
+            for (u32 j = 0; j < d->nfopt; ++j) need |= 1u << d->fopt_vertex[j];
+        }
+        stage_nlf(t, g, q, need, d->order == PSM_ORDER_CFL);
+        TSYNC_B(t);
+        return true;
+    }
+    if (k == 2) {  // start vertices of the CFL filter plan and of the CFL order
+        if (t.rank() == 0) {
             // matching/GenerateFilteringPlan.cpp:343-385: lowest count/degree
             // among the kept options, first one on ties.
-            double best = (double)d->fopt_max_score_num;
-            u32 pick = 0;
-            for (u32 k = 0; k < d->nfopt; ++k) {
-                u32 u = d->fopt_vertex[k];
-                double s = (double)q.item_cnt[u] / (double)d->deg[u];
-                if (s < best) best = s, pick = k;
-            }
-            q.froot = pick;
-        }
-        if (d->order == PSM_ORDER_CFL) {
-            double best = (double)d->fopt_max_score_num;
-            u32 pick = 0;
-            for (u32 k = 0; k < d->noopt; ++k) {
-                u32 u = d->oopt_vertex[k];
-                double s = (double)q.item_cnt[d->oopt_item[k]] / (double)d->deg[u];
-                if (s < best) best = s, pick = k;
-            }
-            q.oroot = pick;
-        }
-    }
-    TSYNC(t);
-    if (!cfl) {
-        // NLFFilter / GQLFilter stop at the first empty set.
-        for (u32 u = 0; u < n; ++u) {
-            if (!compact_vertex(t, g, q, u)) return;
-            TSYNC(t);
-        }
-        if (t.rank() == 0) {
-            for (u32 u = 0; u < n; ++u)
-                if (q.cnt[u] == 0) {
-                    q.empty = 1;
-                    q.filter_ok = 0;
-                    for (u32 v = u + 1; v < n; ++v) q.cnt[v] = 0;
-                    break;
+            if (cfl) {
+                double best = (double)d->fopt_max_score_num;
+                u32 pick = 0;
+                for (u32 j = 0; j < d->nfopt; ++j) {
+                    u32 u = d->fopt_vertex[j];
+                    double s = (double)q.item_cnt[u] / (double)d->deg[u];
+                    if (s < best) best = s, pick = j;
                 }
+                q.froot = pick;
+            }
+            if (d->order == PSM_ORDER_CFL) {
+                double best = (double)d->fopt_max_score_num;
+                u32 pick = 0;
+                for (u32 j = 0; j < d->noopt; ++j) {
+                    u32 u = d->oopt_vertex[j];
+                    double s = (double)q.item_cnt[d->oopt_item[j]] / (double)d->deg[u];
+                    if (s < best) best = s, pick = j;
+                }
+                q.oroot = pick;
+            }
         }
-        TSYNC(t);
-        if (q.empty) return;
+        TSYNC_B(t);
+        return true;
+    }
+    u32 j = k - 3;
+    if (!cfl) {
+        if (j < n) {  // compact u (NLF result)
+            if (!compact_vertex(t, g, q, j)) return false;
+            TSYNC_B(t);
+            return true;
+        }
+        j -= n;
+        if (j == 0) {  // NLFFilter / GQLFilter stop at the first empty set
+            if (t.rank() == 0) {
+                for (u32 u = 0; u < n; ++u)
+                    if (q.cnt[u] == 0) {
+                        q.empty = 1;
+                        q.filter_ok = 0;
+                        for (u32 v = u + 1; v < n; ++v) q.cnt[v] = 0;
+                        break;
+                    }
+            }
+            TSYNC_B(t);
+            return true;
+        }
+        j -= 1;
         if (d->filter == PSM_FILTER_GQL) {
-            for (u32 round = 0; round < 2; ++round)
-                for (u32 u = 0; u < n; ++u) {
+            if (j < 2 * n) {  // refine (round j / n) of u = j % n
+                const u32 u = j % n;
+                if (!q.empty) {
                     const u32 base = bucket_base(g, d->label[u]);
                     const u32 N = q.cnt[u];
                     for (u32 i = t.warp(); i < N; i += t.nwarps()) {
@@ -888,45 +1048,163 @@ __device__ void prepare_query(Team& t, const DevGraph& g, QState& q, DevArena* a
                         if (!gql_check(g, d, q, u, v) && lane_id() == 0)
                             atomicAnd(q.bm[u] + (pos >> 5), ~(1u << (pos & 31u)));
                     }
-                    TSYNC(t);
                 }
-            for (u32 u = 0; u < n; ++u) {
-                if (!compact_vertex(t, g, q, u)) return;
-                TSYNC(t);
+                TSYNC_B(t);
+                return true;
             }
+            j -= 2 * n;
+            if (j < n) {
+                if (!q.empty && !compact_vertex(t, g, q, j)) return false;
+                TSYNC_B(t);
+                return true;
+            }
+            j -= n;
         }
     } else {
         const FilterPlan& fp = d->fplan[q.froot];
-        const u32 r = fp.root;
-        if (!compact_vertex(t, g, q, r)) return;
-        TSYNC(t);
-        for (u32 s = 0; s < fp.nsteps; ++s) {
-            bool ok = fp.step_kind[s] == STEP_GEN ? step_generate(t, g, q, fp.step_u[s], fp.step_mask[s])
-                                                  : step_prune(t, g, q, fp.step_u[s], fp.step_mask[s]);
-            if (!ok) return;
+        if (j == 0) {
+            if (!compact_vertex(t, g, q, fp.root)) return false;
+            TSYNC_B(t);
+            return true;
         }
+        j -= 1;
+        if (j < fp.nsteps)
+            return fp.step_kind[j] == STEP_GEN ? step_generate(t, g, q, fp.step_u[j], fp.step_mask[j])
+                                               : step_prune(t, g, q, fp.step_u[j], fp.step_mask[j]);
+        j -= fp.nsteps;
     }
-    if (t.rank() == 0) {
-        for (u32 u = 0; u < n; ++u)
-            if (q.cnt[u] == 0) q.empty = 1;
+    // tail: empty check, tables, order, enumeration plan
+    if (j == 0) {
+        if (t.rank() == 0)
+            for (u32 u = 0; u < n; ++u)
+                if (q.cnt[u] == 0) q.empty = 1;
+        TSYNC_B(t);
+        return true;
     }
-    TSYNC(t);
-    if (!stage_tables(t, g, q, arena)) return;
-    if (q.adj == nullptr) return;
-    if (d->order == PSM_ORDER_CFL) {
-        const u32* pw = d->plan_words + d->oplan_off[q.oroot];
-        if (!cfl_estimates(t, q, pw)) return;
-        TSYNC(t);
-        if (t.rank() == 0) cfl_order_select(q, pw);
+    const bool skip = !q.filter_ok;  // GQL / NLF early exit: nothing more is built
+    if (j == 1) {
+        if (!skip && !stage_tables(t, g, q, arena)) return false;
+        TSYNC_B(t);
+        return true;
+    }
+    if (j == 2) {
+        if (!skip && q.adj != nullptr) {
+            if (d->order == PSM_ORDER_CFL) {
+                const u32* pw = d->plan_words + d->oplan_off[q.oroot];
+                if (!cfl_estimates(t, q, pw)) return false;
+                TSYNC_B(t);
+                if (t.rank() == 0) cfl_order_select(q, pw);
+            } else if (t.rank() == 0) {
+                gql_order(g, q);
+            }
+        }
+        TSYNC_B(t);
+        return true;
+    }
+    if (t.warp() == 0 && !skip && q.adj != nullptr) enum_plan_warp(g, q);
+    TSYNC_B(t);
+    return true;
+}
+
+// Whether step k is small enough for one block (decided on current counts).
+__device__ bool step_small(const DevGraph& g, const QState& q, u32 k) {
+    constexpr u32 SMALL_ITEMS = 4096;   // candidates / rows handled by one block
+    constexpr u32 SMALL_WORDS = 2048;   // bitmap words handled by one block
+    const QDesc* d = q.desc;
+    const u32 n = d->n;
+    if (k == 1) {
+        u32 words = 0;
+        for (u32 it = 0; it < n + d->nvirt; ++it) words += (bucket_size(g, d->item_label[it]) + 31u) >> 5;
+        return words <= SMALL_WORDS;
+    }
+    if (k == 0 || k == 2) {
+        u32 words = 0;
+        for (u32 u = 0; u < n; ++u) words += q.bwords[u];
+        return k == 2 || words <= 4 * SMALL_WORDS;
+    }
+    u32 j = k - 3;
+    if (!is_cfl(d)) {
+        if (j < n) return q.bwords[j] <= SMALL_WORDS;
+        j -= n;
+        if (j == 0) return true;
+        j -= 1;
+        if (d->filter == PSM_FILTER_GQL) {
+            if (j < 2 * n) return q.cnt[j % n] <= SMALL_ITEMS / 8;
+            j -= 2 * n;
+            if (j < n) return q.bwords[j] <= SMALL_WORDS;
+            j -= n;
+        }
     } else {
-        if (t.rank() == 0) gql_order(g, q);
+        const FilterPlan& fp = d->fplan[q.froot];
+        if (j == 0) return q.bwords[fp.root] <= SMALL_WORDS;
+        j -= 1;
+        if (j < fp.nsteps) {
+            const u32 u = fp.step_u[j];
+            if (q.bwords[u] > SMALL_WORDS) return false;
+            if (fp.step_kind[j] == STEP_PRUNE) return q.cnt[u] <= SMALL_ITEMS;
+            u32 work = 0, m = fp.step_mask[j];
+            while (m) {
+                work += q.cnt[__ffs(m) - 1];
+                m &= m - 1;
+            }
+            return work <= SMALL_ITEMS;
+        }
+        j -= fp.nsteps;
     }
-    TSYNC(t);
-    if (t.rank() == 0) {
-        enum_plan(g, q);
-        if (q.empty) q.root_cnt = 0;
+    if (j == 1) {  // tables: all rows of all directed edges
+        u32 rows = 0;
+        for (u32 x = 0; x < n; ++x) rows += q.cnt[x] * (d->e_first[x + 1] - d->e_first[x]);
+        return rows <= SMALL_ITEMS;
     }
-    TSYNC(t);
+    if (j == 2) {
+        u32 rows = 0;
+        for (u32 x = 0; x < n; ++x) rows += q.cnt[x];
+        return rows <= 4 * SMALL_ITEMS;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void trace_step(QState& q, u32 k) {
+    if (q.trace && k < PSM_TRACE_STEPS) q.trace[k] = global_timer_ns();
+}
+
+template <class Team>
+__device__ void prepare_query(Team& t, const DevGraph& g, QState& q, DevArena* arena) {
+    if (t.rank() == 0 && q.trace) q.trace[PSM_TRACE_STEPS] = global_timer_ns();
+    for (u32 k = 0; k < step_count(q); ++k) {
+        if (!run_step(t, g, q, arena, k)) return;
+        if (t.rank() == 0) trace_step(q, k);
+    }
+}
+
+// Plain path with the whole grid: block 0 runs consecutive small steps on
+// its own (block barriers only); the grid joins for large steps. The other
+// blocks wait at one grid barrier per run of small steps.
+__device__ void prepare_query_hybrid(GridTeam& gt, const DevGraph& g, QState& q, DevArena* arena) {
+    __shared__ u32 s_k;
+    u32 k = 0;
+    if (gt.rank() == 0 && q.trace) q.trace[PSM_TRACE_STEPS] = global_timer_ns();
+    while (true) {
+        if (blockIdx.x == 0) {
+            BlockTeam bt;
+            // Steps 0 and 1 (before the start vertex is picked) always
+            // qualify by size alone.
+            while (k < (k < 3 ? 3u : step_count(q)) && step_small(g, q, k)) {
+                if (!run_step(bt, g, q, arena, k)) break;
+                if (threadIdx.x == 0) trace_step(q, k);
+                ++k;
+            }
+            if (threadIdx.x == 0) q.step_cursor = k;
+        }
+        if (!gt.sync()) return;
+        if (threadIdx.x == 0) s_k = ld_volatile_u32(&q.step_cursor);
+        __syncthreads();
+        k = s_k;
+        if (k >= 3 && k >= step_count(q)) break;
+        if (!run_step(gt, g, q, arena, k)) return;
+        if (gt.rank() == 0) trace_step(q, k);
+        ++k;
+    }
 }
 
 // Batched / serving preparation: blocks take queries from a ticket counter.
@@ -945,11 +1223,20 @@ __global__ void __launch_bounds__(512) prep_block_kernel(DevGraph g, QState* qs,
     }
 }
 
+// Plain path: one query prepared by one thread-block cluster.
+__global__ void __launch_bounds__(512) prep_cluster_kernel(DevGraph g, QState* qs, DevArena* arena) {
+    ClusterTeam t;
+    prepare_query(t, g, qs[0], arena);
+}
+
 // Plain path: one query prepared by the whole (co-resident) grid.
 __global__ void __launch_bounds__(512) prep_grid_kernel(DevGraph g, QState* qs, GridBarrier* bar, DevArena* arena,
                                                         u64 budget_ns) {
     GridTeam t{bar, global_timer_ns() + budget_ns};
-    prepare_query(t, g, qs[0], arena);
+    if (qs[0].step_cursor == HYBRID_REQUEST)
+        prepare_query_hybrid(t, g, qs[0], arena);
+    else
+        prepare_query(t, g, qs[0], arena);
 }
 
 }  // namespace
@@ -967,6 +1254,49 @@ cudaError_t psm_launch_prep_grid(const DevGraph& g, QState* qs, void* barrier, D
     GridBarrier* bar = (GridBarrier*)barrier;
     void* args[] = {(void*)&g, (void*)&qs, (void*)&bar, (void*)&arena, (void*)&budget_ns};
     return cudaLaunchCooperativeKernel((const void*)prep_grid_kernel, dim3(blocks), dim3(threads), args, 0, st);
+}
+
+// Largest supported cluster size (<= want) for the cluster preparation kernel.
+cudaError_t psm_prep_cluster_size(int threads, int want, int* size) {
+    cudaError_t e = cudaFuncSetAttribute(prep_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+    for (int cs = want; cs >= 1; cs >>= 1) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = cs;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(threads);
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        e = cudaOccupancyMaxActiveClusters(&clusters, prep_cluster_kernel, &cfg);
+        if (e == cudaSuccess && clusters > 0) {
+            *size = cs;
+            return cudaSuccess;
+        }
+        cudaGetLastError();
+    }
+    *size = 1;
+    return cudaSuccess;
+}
+
+cudaError_t psm_launch_prep_cluster(const DevGraph& g, QState* qs, DevArena* arena, int cluster, int threads,
+                                    cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cluster);
+    cfg.blockDim = dim3(threads);
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, prep_cluster_kernel, g, qs, arena);
 }
 
 cudaError_t psm_prep_grid_max_blocks(int threads, int* blocks) {

@@ -22,6 +22,8 @@
 #define PSM_MAXOPT 3         // start-vertex options kept by the CFL rank heap
 #define PSM_MAXDIR 992       // directed query edges (32 * 31)
 #define PSM_PLAN_WORDS 4096  // CFL order plan blob capacity (u32 words)
+#define PSM_TRACE_STEPS 256  // preparation steps recorded when tracing (+1 start stamp)
+#define HYBRID_REQUEST 0xFFFFFFFFu  // QState.step_cursor on entry: use the hybrid grid driver
 
 typedef uint32_t u32;
 typedef uint64_t u64;
@@ -83,6 +85,7 @@ struct QDesc {
     // e_first[x] .. e_first[x+1]-1 with targets in ascending order.
     u32 e_first[PSM_MAXQ + 1];
     u32 e_dst[PSM_MAXDIR];
+    u32 e_src[PSM_MAXDIR];
     u32 plan_used;              // words of plan_words in use (last member: only
     u32 plan_words[PSM_PLAN_WORDS];  // the used prefix is copied to the device)
 };
@@ -106,6 +109,7 @@ struct QState {
     u32 item_cnt[PSM_MAXQ + PSM_MAXOPT];
     u32* acc;               // CFL accumulator bitmap (max bwords)
     u32* tmp;               // CFL per-pivot bitmap
+    u32 acc_words;          // words of acc / tmp
     // tables: row counts / offsets for all directed edges, concatenated
     u32* P;                 // [total_rows + 1] absolute offsets into adj
     u32 e_row_base[PSM_MAXDIR + 1];
@@ -114,11 +118,14 @@ struct QState {
     u32 adj_cap;            // words available at adj (set by the allocator)
     // scratch for team scans / estimates
     u32* scan;              // >= team warps + 1 words
-    u64* est_a;             // >= max candidate count
-    u64* est_b;
+    u64* est_a;             // est_blocks x 2 x est_stride path-estimate buffers
+    u32 est_stride;         // >= max candidate count
+    u32 est_blocks;         // blocks that estimate paths concurrently
     u64* est_out;           // per path estimates (<= PSM_PLAN_WORDS)
     // plan
     u32 froot, oroot;
+    u32 step_cursor;        // next preparation step (hybrid grid driver)
+    u64* trace;             // optional: %globaltimer at the end of each step
     u32 order[PSM_MAXQ];
     u32 pivot[PSM_MAXQ];
     u32 empty;              // some candidate set is empty -> count 0
