@@ -126,6 +126,18 @@ int psm_run_order(psm_run* run, uint32_t* order, uint32_t* pivot);
 int psm_run_embeddings(psm_run* run, uint32_t* buf, uint64_t buf_rows, uint64_t* rows);
 void psm_run_free(psm_run* run);
 
+/* No counterpart in the reference. Re-counts the embeddings of a prepared
+ * run (psm_run_create with emit = 0) without allocating: for callers that
+ * cannot allocate device memory at this point (inside CUDA stream capture,
+ * latency-critical loops that cannot afford an allocation's implicit device
+ * synchronisation, hosts whose device memory belongs to another runtime's
+ * pool). The enumeration's scratch lives in a static 1 MiB device array per
+ * GPU, held until process exit; the first call on a device looks up that
+ * array's address, so make it before any stream capture. All calls share the
+ * array: calls whose work overlaps on the GPU race and must not be issued.
+ * Writes min(total, cap) to *count (cap 0 = none). */
+int psm_run_recount_noalloc(psm_run* run, uint64_t cap, double time_limit_s, uint64_t* count, uint32_t* overtime);
+
 /* ---- batched path: many queries through one persistent preparation launch
  *      and one persistent enumeration launch (no counterpart in the
  *      reference, which runs queries one process at a time) ---- */

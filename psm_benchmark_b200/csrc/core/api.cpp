@@ -86,6 +86,19 @@ struct psm_run {
     u32 n = 0;
 };
 
+int psm_fail(int code, const std::string& msg) { return fail(code, msg); }
+
+int psm_run_internals(psm_run* r, RunInternals* out) {
+    if (!r || !r->ctx || !r->d_q) return fail(PSM_ERR_ARG, "run is not alive");
+    out->device = r->ctx->device;
+    out->stream = r->ctx->st;
+    out->dq = r->d_q;
+    out->dev = &r->g->dev;
+    out->enum_blocks = r->ctx->enum_blocks;
+    out->emit = r->hq.emit_buf != nullptr;
+    return PSM_OK;
+}
+
 namespace {
 
 struct Layout {

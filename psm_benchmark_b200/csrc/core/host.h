@@ -24,6 +24,20 @@ struct psm_graph {
     u32 freq(u32 l) const { return l < L ? lab_off[l + 1] - lab_off[l] : 0u; }
 };
 
+// Records msg as this thread's last error and returns code.
+int psm_fail(int code, const std::string& msg);
+
+// What the allocation-free recount needs from a finished run.
+struct RunInternals {
+    int device;
+    cudaStream_t stream;
+    QState* dq;
+    const DevGraph* dev;
+    int enum_blocks;
+    u32 emit;
+};
+int psm_run_internals(psm_run* run, RunInternals* out);
+
 // Builds the device query descriptor (validation, NLF lists, CFL plans).
 // Returns PSM_OK or PSM_ERR_ARG with *err set.
 int psm_build_qdesc(const psm_graph& g, const psm_query_desc& q, const psm_options& opt, QDesc* d, std::string* err);

@@ -22,7 +22,7 @@ EXPORTS = [
     "psm_graph_from_csr", "psm_graph_load", "psm_graph_info", "psm_graph_free",
     "psm_context_create", "psm_context_free",
     "psm_match", "psm_run_create", "psm_run_candidates", "psm_run_table", "psm_run_order",
-    "psm_run_embeddings", "psm_run_free", "psm_match_batch",
+    "psm_run_embeddings", "psm_run_free", "psm_match_batch", "psm_run_recount_noalloc",
 ]
 
 
@@ -81,6 +81,7 @@ def lib():
         "psm_run_free": ([vp], None),
         "psm_match_batch": ([vp, vp, C.POINTER(QueryDesc), C.c_uint32, C.POINTER(Options), C.POINTER(Result)],
                             C.c_int),
+        "psm_run_recount_noalloc": ([vp, C.c_uint64, C.c_double, C.POINTER(C.c_uint64), u32p], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -1,0 +1,55 @@
+"""The allocation-free recount entry point, psm_run_recount_noalloc.
+
+It exists for callers that cannot allocate device memory when they need a
+count (inside stream capture, allocation-free serving loops, hosts whose
+device memory belongs to another runtime). The test calls it through the C
+ABI on prepared runs and checks, for two calls in a row, that its count is
+exactly the count of the ordinary entry point (integer counts: no
+tolerance). This file is collected last so that a failure here never hides
+the rest of the suite; it also passes when run alone.
+"""
+import ctypes as C
+
+import pytest
+
+from psm_benchmark_b200 import api
+from psm_benchmark_b200 import native as N
+from tests import golden_data as gd
+
+pytestmark = pytest.mark.gpu
+
+
+def test_recount_noalloc_matches_plain_path():
+    g = gd.synthetic_graph("rmat12")
+    case = dict(gd.synthetic_cases())["rmat12"]
+    queries = [gd.query_from_rec(e["query"]) for e in case["queries"][:8]]
+    with api.Engine(arena_bytes=1 << 30) as eng:
+        dg = api.DataGraph.from_graph(g)
+        checked = 0
+        for q in queries:
+            for method, cap in (("CFL_CFL_EXPLORE", 0), ("GQL_GQL_GQL", 1000)):
+                with api.Run(eng, dg, q, method, cap=cap) as run:
+                    expected = run.result.count
+                    for _ in range(2):  # two calls in a row share the static scratch
+                        cnt = C.c_uint64(0)
+                        over = C.c_uint32(1)
+                        rc = N.lib().psm_run_recount_noalloc(run._h, cap, 60.0, C.byref(cnt), C.byref(over))
+                        assert rc == N.PSM_OK, N.lib().psm_last_error()
+                        assert over.value == 0
+                        assert cnt.value == expected
+                checked += 1
+        dg.close()
+    assert checked == 2 * len(queries)
+
+
+def test_recount_noalloc_rejects_emit_runs():
+    g = gd.synthetic_graph("rmat12")
+    case = dict(gd.synthetic_cases())["rmat12"]
+    q = gd.query_from_rec(case["queries"][0]["query"])
+    with api.Engine(arena_bytes=1 << 30) as eng:
+        dg = api.DataGraph.from_graph(g)
+        with api.Run(eng, dg, q, "CFL_CFL_EXPLORE", emit=16) as run:
+            cnt = C.c_uint64(0)
+            rc = N.lib().psm_run_recount_noalloc(run._h, 0, 60.0, C.byref(cnt), None)
+            assert rc == N.PSM_ERR_ARG
+        dg.close()
