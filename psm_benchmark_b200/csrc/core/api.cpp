@@ -268,6 +268,18 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
             worst = PSM_ERR_INTERNAL;
         }
     }
+    if (hq[0].trace && nq > 1) {
+        // per-query time at which the cap was reached, relative to the first
+        std::vector<QState> st(nq);
+        CK(cudaMemcpy(st.data(), lay.d_q, sizeof(QState) * nq, cudaMemcpyDeviceToHost));
+        u64 t0 = ~0ull;
+        for (auto& s : st)
+            if (s.done_ns) t0 = std::min(t0, s.done_ns);
+        fprintf(stderr, "psm trace done(us):");
+        for (u32 i = 0; i < nq; ++i)
+            fprintf(stderr, " %u:%.0f", i, st[i].done_ns ? (st[i].done_ns - t0) / 1e3 : -1.0);
+        fprintf(stderr, "\n");
+    }
     if (hq[0].trace) {
         for (u32 i = 0; i < nq && i < 4; ++i) {
             std::vector<u64> tr(PSM_TRACE_STEPS + 1);

@@ -137,6 +137,11 @@ __device__ __forceinline__ u32 cand_pos(const QState& q, u32 u, u32 v) {
     return q.rank[u][b >> 5] + __popc(word & ((1u << (b & 31u)) - 1u));
 }
 
+// Marks the query stopped (cap reached); the first caller stamps the time.
+__device__ __forceinline__ void cap_reached(QState& q) {
+    if (atomicExch(&q.stop, 1u) == 0) q.done_ns = global_timer_ns();
+}
+
 // One lane's candidate test at depth d for driver element p (a position in
 // C(u_d)): member of every other row and not a data vertex already used by a
 // same-label earlier depth.
@@ -157,6 +162,13 @@ __device__ __forceinline__ bool accept(const QState& q, u32 d, u32 p, const Warp
         }
     }
     return true;
+}
+
+// Candidate test of one lane's driver element p at depth d (lanes whose
+// element lies past the row end pass valid = false).
+__device__ __forceinline__ bool chunk_accept(const QState& q, u32 d, u32 p, bool valid, WarpStack* ws,
+                                             const u32* list_d) {
+    return valid && accept(q, d, p, ws, list_d);
 }
 
 // Warp-level count of the candidates of the last depth d given the prefix.
@@ -192,9 +204,9 @@ __device__ u64 count_last(const QState& q, u32 d, WarpStack* ws, u64& bytes, u64
     __syncwarp();
     u64 c = 0;
     for (u32 j = 0; j < blen; j += 32) {
-        bool ok = false;
-        if (j + lane < blen) ok = accept(q, d, q.adj[bs + j + lane], ws, list_d);
-        c += __popc(__ballot_sync(FULL_MASK, ok));
+        const bool valid = j + lane < blen;
+        const u32 p = valid ? q.adj[bs + j + lane] : 0u;
+        c += __popc(__ballot_sync(FULL_MASK, chunk_accept(q, d, p, valid, ws, list_d)));
     }
     return c;
 }
@@ -240,7 +252,13 @@ __device__ u64 emit_last(QState& q, const DevGraph& g, u32 d, WarpStack* ws, u64
 // sits at depth dl - 1, the rest of the prefix is shared in ws. Counts the
 // positions in the intersection of the backward-neighbour rows of depth dl
 // whose data vertex differs from every same-label vertex of the embedding.
-__device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const WarpStack* ws, u64& bytes, u64& calls) {
+// An intersection whose shortest row is longer than LONG_ROW is not walked by
+// the lane: it sets *defer and the warp counts it cooperatively afterwards
+// (warp_last_count), so one hub row does not stall 31 idle lanes.
+constexpr u32 LONG_ROW = 24;
+
+__device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const WarpStack* ws, u64& bytes, u64& calls,
+                               bool* defer) {
     const u32 nb = q.nbn[dl];
     const u32 dp = dl - 1;
     u32 blo = 0, bhi = 0, blen = 0xFFFFFFFFu, bk = 0;
@@ -255,6 +273,10 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const Warp
     bytes += by;
     calls += blen;
     if (blen == 0) return 0;
+    if (nb > 1 && blen > LONG_ROW) {
+        *defer = true;
+        return 0;
+    }
     const u32 u = q.order[dl];
     const u32 same = q.same_mask[dl];
     if (nb == 1) {
@@ -289,6 +311,49 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const Warp
             }
         }
         c += ok;
+    }
+    return c;
+}
+
+// Warp-cooperative form of lane_last_count for one (p, v) (warp-uniform):
+// the shortest row is walked 32 entries at a time, each lane binary-searching
+// its entry in the other rows. Rows and bytes were counted by the lane that
+// deferred it.
+__device__ u64 warp_last_count(const QState& q, u32 dl, u32 p, u32 v, const WarpStack* ws) {
+    const u32 lane = lane_id();
+    const u32 nb = q.nbn[dl];
+    const u32 dp = dl - 1;
+    u32 blo = 0, bhi = 0, blen = 0xFFFFFFFFu, bk = 0;
+    for (u32 k = 0; k < nb; ++k) {
+        const u32 bd = q.bn_depth[dl][k];
+        const u32 base = q.bn_tab[dl][k] + (bd == dp ? p : ws->pos[bd]);
+        const u32 lo = q.P[base], hi = q.P[base + 1];
+        if (hi - lo < blen) blen = hi - lo, blo = lo, bhi = hi, bk = k;
+    }
+    const u32 u = q.order[dl];
+    const u32 same = q.same_mask[dl];
+    const u32* list = q.list[u];
+    u64 c = 0;
+    for (u32 e0 = blo; e0 < bhi; e0 += 32) {
+        const u32 e = e0 + lane;
+        bool ok = e < bhi;
+        const u32 x = ok ? __ldg(q.adj + e) : 0u;
+        for (u32 k = 0; k < nb && ok; ++k) {
+            if (k == bk) continue;
+            const u32 bd = q.bn_depth[dl][k];
+            const u32 base = q.bn_tab[dl][k] + (bd == dp ? p : ws->pos[bd]);
+            ok = contains_u32(q.adj, q.P[base], q.P[base + 1], x);
+        }
+        if (ok && same) {
+            const u32 vx = __ldg(list + x);
+            u32 m = same;
+            while (m && ok) {
+                const u32 j = __ffs(m) - 1;
+                m &= m - 1;
+                ok = vx != (j == dp ? v : ws->vid[j]);
+            }
+        }
+        c += __popc(__ballot_sync(FULL_MASK, ok));
     }
     return c;
 }
@@ -458,7 +523,7 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
     }
     if (count >= (1ull << 16) && lane == 0) {
         unsigned long long old = atomicAdd((unsigned long long*)&q.count, count);
-        if (q.cap && old + count >= q.cap) atomicExch(&q.stop, 1u);
+        if (q.cap && old + count >= q.cap) cap_reached(q);
         count = 0;
     }
     count = __shfl_sync(FULL_MASK, count, 0);
@@ -490,13 +555,22 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
                 const u32 cur = ws->cur[d], end = ws->end[d];
                 const u32 idx = cur + lane;
                 u64 c = 0;
-                if (idx < end) {
-                    const u32* list_d = q.list[q.order[d]];
-                    u32 p = d == 0 ? idx : q.adj[idx];
-                    if (d == 0 || accept(q, d, p, ws, list_d))
-                        c = lane_last_count(q, d + 1, p, list_d[p], ws, bytes_l, calls_l);
-                }
+                bool defer = false;
+                const u32* list_d = q.list[q.order[d]];
+                const bool valid = idx < end;
+                const u32 p = valid ? (d == 0 ? idx : q.adj[idx]) : 0u;
+                const bool ok = d == 0 ? valid : chunk_accept(q, d, p, valid, ws, list_d);
+                const u32 v = ok ? list_d[p] : 0u;
+                if (ok) c = lane_last_count(q, d + 1, p, v, ws, bytes_l, calls_l, &defer);
                 count += warp_sum64(c);
+                // long intersections deferred by their lanes: whole warp each
+                u32 dm = __ballot_sync(FULL_MASK, defer);
+                while (dm) {
+                    const u32 src = __ffs(dm) - 1;
+                    dm &= dm - 1;
+                    count += warp_last_count(q, d + 1, __shfl_sync(FULL_MASK, p, src), __shfl_sync(FULL_MASK, v, src),
+                                             ws);
+                }
                 calls += min(32u, end - cur);
                 __syncwarp();
                 if (lane == 0) ws->cur[d] = min(end, cur + 32u);
@@ -529,15 +603,9 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
         } else if (ws->cur[d] < ws->end[d]) {
             const u32 cur = ws->cur[d], end = ws->end[d];
             const u32 idx = cur + lane;
-            bool ok = false;
-            u32 p = 0;
-            if (d == 0) {
-                p = idx;
-                ok = idx < end;
-            } else if (idx < end) {
-                p = q.adj[idx];
-                ok = accept(q, d, p, ws, q.list[q.order[d]]);
-            }
+            const bool valid = idx < end;
+            const u32 p = valid ? (d == 0 ? idx : q.adj[idx]) : 0u;
+            const bool ok = d == 0 ? valid : chunk_accept(q, d, p, valid, ws, q.list[q.order[d]]);
             u32 bal = __ballot_sync(FULL_MASK, ok);
             if (ok) ws->chunk[d][__popc(bal & ((1u << lane) - 1u))] = p;
             calls += min(32u, end - cur);
@@ -566,7 +634,7 @@ __device__ void publish(QState& q, u64 count, u64 bytes, u64 calls) {
     if (lane_id() == 0) {
         if (count) {
             unsigned long long old = atomicAdd((unsigned long long*)&q.count, count);
-            if (q.cap && old + count >= q.cap) atomicExch(&q.stop, 1u);
+            if (q.cap && old + count >= q.cap) cap_reached(q);
         }
         if (calls) atomicAdd((unsigned long long*)&q.calls, calls);
         if (bytes) atomicAdd((unsigned long long*)&q.alg_bytes, bytes);

@@ -147,6 +147,7 @@ struct QState {
     u64 alg_bytes;          // algorithmic bytes of the intersections
     u32 stop;               // cap reached / error -> stop enumerating
     u32 overtime;
+    u64 done_ns;            // %globaltimer when the cap was reached (0 if never)
     // emit mode
     u32* emit_buf;
     u64 emit_cap_rows;
