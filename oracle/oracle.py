@@ -48,6 +48,8 @@ def _lib():
     lib.orc_res_table.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, u32p, u32p]
     lib.orc_res_order.argtypes = [C.c_void_p, u32p, u32p]
     lib.orc_res_emb.argtypes = [C.c_void_p, u32p]
+    u64p = C.POINTER(C.c_uint64)
+    lib.orc_res_depth_stats.argtypes = [C.c_void_p, u64p, u64p, u64p]
     lib.orc_res_free.argtypes = [C.c_void_p]
     return lib
 
@@ -67,6 +69,9 @@ class OracleResult:
     order: np.ndarray
     pivot: np.ndarray
     embeddings: np.ndarray    # [n_emb, q] data ids in query-vertex order
+    depth_nodes: np.ndarray = None  # per depth: partial embeddings accepted
+    depth_cands: np.ndarray = None  # per depth: candidates examined
+    depth_bytes: np.ndarray = None  # per depth: algorithmic bytes of table rows read
 
 
 class OracleGraph:
@@ -111,9 +116,12 @@ class OracleGraph:
             emb = np.empty((ne, n), np.uint32)
             if ne:
                 lib.orc_res_emb(r, _p(emb))
+            stats = [np.zeros(n, np.uint64) for _ in range(3)]
+            lib.orc_res_depth_stats(r, *[a.ctypes.data_as(C.POINTER(C.c_uint64)) for a in stats])
             return OracleResult(count=int(lib.orc_res_count(r)), calls=int(lib.orc_res_calls(r)),
                                 memory_bytes=int(lib.orc_res_memory(r)), filter_ok=bool(lib.orc_res_filter_ok(r)),
-                                candidates=cands, tables=tables, order=order_, pivot=pivot, embeddings=emb)
+                                candidates=cands, tables=tables, order=order_, pivot=pivot, embeddings=emb,
+                                depth_nodes=stats[0], depth_cands=stats[1], depth_bytes=stats[2])
         finally:
             lib.orc_res_free(r)
 

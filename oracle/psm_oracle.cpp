@@ -651,6 +651,9 @@ struct Enumerator {
     u64 cap, count = 0, calls = 0;
     u64 emit_limit;
     std::vector<u32>* emit;
+    // Per depth: partial embeddings accepted, candidates examined and
+    // algorithmic bytes of the table rows read (8 B of offsets + 4 B per entry).
+    std::vector<u64> depth_nodes, depth_cands, depth_bytes;
 
     Enumerator(const Graph& q, const Cands& c, const std::vector<std::vector<Table>>& t, const std::vector<u32>& o,
                u64 cap_, u64 emit_limit_, std::vector<u32>* emit_)
@@ -667,6 +670,9 @@ struct Enumerator {
         emb_pos.assign(Q.n, 0);
         emb_vid.assign(Q.n, INVALID);
         buf.assign(Q.n, {});
+        depth_nodes.assign(Q.n, 0);
+        depth_cands.assign(Q.n, 0);
+        depth_bytes.assign(Q.n, 0);
     }
 
     bool used(u32 v) const {
@@ -686,6 +692,11 @@ struct Enumerator {
         const Table& t0 = T[bn[d][0]][u];
         u32 r0 = emb_pos[bn[d][0]];
         out.assign(t0.adj.begin() + t0.off[r0], t0.adj.begin() + t0.off[r0 + 1]);
+        for (u32 b : bn[d]) {
+            const Table& t = T[b][u];
+            u32 r = emb_pos[b];
+            depth_bytes[d] += 8 + 4ull * (t.off[r + 1] - t.off[r]);
+        }
         std::vector<u32> tmp;
         for (size_t i = 1; i < bn[d].size(); ++i) {
             const Table& t = T[bn[d][i]][u];
@@ -704,7 +715,9 @@ struct Enumerator {
         for (u32 p : buf[d]) {
             u32 v = C[u][p];
             ++calls;
+            ++depth_cands[d];
             if (used(v)) continue;
+            ++depth_nodes[d];
             if (d + 1 == Q.n) {
                 ++count;
                 if (emit && count <= emit_limit) {
@@ -731,6 +744,7 @@ struct Result {
     Cands C;
     std::vector<std::vector<Table>> T;
     std::vector<u32> order, pivot, emb;
+    std::vector<u64> depth_nodes, depth_cands, depth_bytes;
 };
 
 Graph make_graph(const u32* off, const u32* adj, const u32* lab, u32 n) {
@@ -785,6 +799,9 @@ void* orc_run(void* gp, const u32* qoff, const u32* qadj, const u32* qlab, u32 q
         e.dfs(0);
         r->count = cap && e.count > cap ? cap : e.count;
         r->calls = e.calls;
+        r->depth_nodes = e.depth_nodes;
+        r->depth_cands = e.depth_cands;
+        r->depth_bytes = e.depth_bytes;
     }
     return r;
 }
@@ -793,6 +810,17 @@ u64 orc_res_count(void* r) { return ((Result*)r)->count; }
 u64 orc_res_calls(void* r) { return ((Result*)r)->calls; }
 u64 orc_res_memory(void* r) { return ((Result*)r)->memory; }
 int orc_res_filter_ok(void* r) { return ((Result*)r)->filter_ok; }
+// Per depth of the matching order (qn entries each): partial embeddings
+// accepted, candidates examined, algorithmic bytes of table rows read.
+// All zero when enumeration did not run.
+void orc_res_depth_stats(void* r, u64* nodes, u64* cands, u64* bytes) {
+    auto* x = (Result*)r;
+    for (size_t d = 0; d < x->depth_nodes.size(); ++d) {
+        nodes[d] = x->depth_nodes[d];
+        cands[d] = x->depth_cands[d];
+        bytes[d] = x->depth_bytes[d];
+    }
+}
 u32 orc_res_cand_count(void* r, u32 u) { return (u32)((Result*)r)->C[u].size(); }
 void orc_res_cands(void* r, u32 u, u32* out) {
     auto& c = ((Result*)r)->C[u];

@@ -67,6 +67,7 @@ struct psm_context {
     void* d_barrier = nullptr;
     u32* d_ticket = nullptr;
     void* d_enum_scratch = nullptr;
+    u32* d_enum_cache = nullptr;  // per-warp prefix-intersection caches (own allocation)
     int prep_threads = 512;
     int prep_grid_blocks = 0;
     int prep_block_blocks = 0;
@@ -236,7 +237,7 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_enum_q, budget, opt.emit ? 1 : 0,
-                       ctx->enum_blocks, ctx->st));
+                       ctx->enum_blocks, ctx->d_enum_cache, ctx->st));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     CK(psm_launch_gather(lay.d_q, nq, lay.d_res, ctx->st));
     std::vector<DevResult> res(nq);
@@ -388,6 +389,18 @@ int psm_context_create(int device, uint64_t arena_bytes, psm_context** out) {
         return fail(PSM_ERR_CUDA, "occupancy query failed");
     }
     c->prep_block_blocks = prop.multiProcessorCount * 4;
+    // PSM_ENUM_CACHE=0 runs the enumerator without prefix-intersection caches.
+    const char* ec = getenv("PSM_ENUM_CACHE");
+    if (!(ec && strcmp(ec, "0") == 0)) {
+        const size_t cb = psm_enum_cache_bytes(c->enum_blocks);
+        e = cudaMalloc((void**)&c->d_enum_cache, cb);
+        // the enumerator keeps its cache bitmaps all-zero between tasks
+        if (e == cudaSuccess) e = cudaMemset(c->d_enum_cache, 0, cb);
+        if (e != cudaSuccess) {
+            psm_context_free(c);
+            return cuda_fail(e, "enumeration cache allocation");
+        }
+    }
     // Plain-path preparation team: the whole grid (default; measured fastest
     // on B200) or one thread-block cluster (PSM_PLAIN_TEAM=cluster,
     // PSM_CLUSTER=size).
@@ -407,6 +420,7 @@ void psm_context_free(psm_context* c) {
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->arena) cudaFree(c->arena);
+    if (c->d_enum_cache) cudaFree(c->d_enum_cache);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
 }

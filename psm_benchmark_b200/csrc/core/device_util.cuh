@@ -26,6 +26,24 @@ __device__ __forceinline__ bool contains_u32(const u32* __restrict__ a, u32 lo, 
     return i < hi && __ldg(a + i) == key;
 }
 
+// Plain-load forms for memory that the running kernel itself writes (the
+// enumerator's per-warp intersection caches): the read-only path behind
+// __ldg may serve lines that are stale for such memory.
+__device__ __forceinline__ u32 lower_bound_rw(const u32* a, u32 lo, u32 hi, u32 key) {
+    while (lo < hi) {
+        u32 mid = (lo + hi) >> 1;
+        if (a[mid] < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+__device__ __forceinline__ bool contains_rw(const u32* a, u32 lo, u32 hi, u32 key) {
+    u32 i = lower_bound_rw(a, lo, hi, key);
+    return i < hi && a[i] == key;
+}
+
 // Range of neighbours of internal vertex v that carry label l.
 __device__ __forceinline__ void label_run(const DevGraph& g, u32 v, u32 l, u32& s, u32& e) {
     u32 lo = g.off[v], hi = g.off[v + 1];

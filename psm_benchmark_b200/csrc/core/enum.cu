@@ -76,7 +76,38 @@ struct EnumCtl {
 
 namespace {
 
+// Level flags (WarpStack::flg). A level in cached mode intersects at most
+// two sorted arrays: the depth's prefix-intersection cache S (the rows of
+// the backward neighbours at depths <= d - 2, intersected once per prefix)
+// and the row R of the backward neighbour at depth d - 1, if any.
+enum : u32 {
+    LV_CACHED = 1,     // cached mode
+    LV_DRV_CACHE = 2,  // the driver range indexes S (else q.adj)
+    LV_OTHER = 4,      // the array that is not the driver is tested: R at [olo, ohi), or S
+    LV_OTHER_BM = 8,   // ... and S is tested through its bitmap
+};
+// Per warp and depth a slot of CACHE_CAP list entries and BM_WORDS bitmap
+// words. A cache whose intersection is longer than CACHE_CAP is not kept;
+// a single cached row stays in q.adj and only its bitmap is built.
+constexpr u32 CACHE_CAP = 512;
+constexpr u32 BM_WORDS = PSM_CACHE_BM_BITS / 32;
+constexpr u32 SLOT_WORDS = CACHE_CAP + BM_WORDS;
+constexpr u32 NO_ROW = 0xFFFFFFFFu;
+constexpr u32 LONG_ROW = 24;     // per-lane binary-search walks longer than this go to the warp
+constexpr u32 LONG_BM_ROW = 96;  // per-lane bitmap walks longer than this go to the warp
+
+// Invariants of the cache state: cvalid bit d => S of depth d is the
+// intersection for the current prefix; cbits bit d => the bitmap of depth d
+// holds exactly the bits of the list S_d (clen[d] entries, in q.adj from
+// clo[d] when cadj bit d, else in the slot). Every bitmap is all-zero while
+// its bit in cbits is clear; run_task clears them all before it returns, so
+// bitmaps start each task (and each launch) empty.
 struct WarpStack {
+    u32* cbuf;          // this warp's slots (null: caching off)
+    u32 cvalid;
+    u32 cover;          // depths whose intersection overflowed CACHE_CAP for the current prefix
+    u32 cbits;
+    u32 cadj;
     u32 pos[PSM_MAXQ];
     u32 vid[PSM_MAXQ];
     u32 cur[PSM_MAXQ];
@@ -84,6 +115,11 @@ struct WarpStack {
     u32 drv[PSM_MAXQ];
     u32 cn[PSM_MAXQ];
     u32 ci[PSM_MAXQ];
+    u32 flg[PSM_MAXQ];
+    u32 olo[PSM_MAXQ];
+    u32 ohi[PSM_MAXQ];
+    u32 clen[PSM_MAXQ];
+    u32 clo[PSM_MAXQ];
     u32 chunk[PSM_MAXQ][32];
 };
 
@@ -103,29 +139,205 @@ __device__ __forceinline__ u32 row_hi(const QState& q, u32 d, u32 k, const u32* 
     return q.P[q.bn_tab[d][k] + pos[q.bn_depth[d][k]] + 1];
 }
 
-// Picks the shortest backward-neighbour row at depth d as the driver and
-// adds the algorithmic bytes of reading all rows.
-__device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws, u64& bytes) {
-    const u32 nb = q.nbn[d];
-    u32 best = 0, blen = 0xFFFFFFFFu, bs = 0;
-    u64 by = 0;
-    for (u32 k = 0; k < nb; ++k) {
-        u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
-        u32 len = hi - lo;
-        by += 8u + 4ull * len;
-        if (len < blen) blen = len, best = k, bs = lo;
+__device__ __forceinline__ u32* slot_list(const WarpStack* ws, u32 d) { return ws->cbuf + d * SLOT_WORDS; }
+__device__ __forceinline__ u32* slot_bm(const WarpStack* ws, u32 d) { return ws->cbuf + d * SLOT_WORDS + CACHE_CAP; }
+// The sorted list S of depth d (valid while cvalid or cbits has bit d).
+__device__ __forceinline__ const u32* cache_list(const QState& q, const WarpStack* ws, u32 d) {
+    return ((ws->cadj >> d) & 1u) ? q.adj + ws->clo[d] : slot_list(ws, d);
+}
+__device__ __forceinline__ bool bm_test(const u32* bm, u32 x) { return (bm[x >> 5] >> (x & 31u)) & 1u; }
+// Membership of candidate position x in S of depth d (bitmap when built).
+__device__ __forceinline__ bool in_cache(const QState& q, const WarpStack* ws, u32 d, u32 x) {
+    if ((ws->cbits >> d) & 1u) return bm_test(slot_bm(ws, d), x);
+    return contains_rw(cache_list(q, ws, d), 0, ws->clen[d], x);
+}
+
+// Clears the bitmap bits of depth d (from its list), if any are set.
+__device__ void clear_bits(const QState& q, WarpStack* ws, u32 d) {
+    if (!((ws->cbits >> d) & 1u)) return;
+    const u32* L = cache_list(q, ws, d);
+    const u32 n = ws->clen[d];
+    u32* bm = slot_bm(ws, d);
+    for (u32 i = lane_id(); i < n; i += 32) bm[L[i] >> 5] = 0u;
+    __syncwarp();
+    if (lane_id() == 0) ws->cbits &= ~(1u << d);
+    __syncwarp();
+}
+
+// Sets the bitmap bits of depth d from its (ascending) list: lanes holding
+// positions of one word OR their bits together and one of them stores, so
+// every word has a single writer per pass.
+__device__ void set_bits(const QState& q, WarpStack* ws, u32 d) {
+    const u32* L = cache_list(q, ws, d);
+    const u32 n = ws->clen[d];
+    u32* bm = slot_bm(ws, d);
+    const u32 lane = lane_id();
+    for (u32 j = 0; j < n; j += 32) {
+        const bool valid = j + lane < n;
+        const u32 x = valid ? L[j + lane] : 0u;
+        const u32 w = valid ? (x >> 5) : 0xFFFFFFFFu;
+        const u32 peers = __match_any_sync(FULL_MASK, w);
+        const u32 bits = __reduce_or_sync(peers, valid ? (1u << (x & 31u)) : 0u);
+        if (valid && lane == (u32)(__ffs(peers) - 1)) bm[w] |= bits;
+        __syncwarp();
     }
-    bytes += by;
+    if (lane == 0) ws->cbits |= 1u << d;
+    __syncwarp();
+}
+
+// Clears every bitmap this warp has set (end of a task).
+__device__ void release_caches(const QState& q, WarpStack* ws) {
+    for (u32 m = ws->cbits; m; m &= m - 1) clear_bits(q, ws, __ffs(m) - 1);
     __syncwarp();
     if (lane_id() == 0) {
+        ws->cvalid = 0;
+        ws->cover = 0;
+        ws->cadj = 0;
+    }
+    __syncwarp();
+}
+
+// Makes the cache S of depth d hold the intersection of the rows q.cmask[d]
+// for the current prefix, building it when needed (one row: kept in place;
+// several: driver = shortest row, one lane per driver entry, ballot
+// compaction into the slot), then its bitmap when the candidate set of the
+// depth is small enough. Returns false when depth d has no cache plan,
+// caching is off, or the intersection has more than CACHE_CAP entries; the
+// level then intersects the table rows directly.
+__device__ bool ensure_cache(const QState& q, u32 d, WarpStack* ws, u64& bytes) {
+    const u32 cm = q.cmask[d];
+    if (cm == 0 || ws->cbuf == nullptr) return false;
+    const u32 bit = 1u << d;
+    if (ws->cvalid & bit) return true;
+    if (ws->cover & bit) return false;
+    clear_bits(q, ws, d);
+    const u32 lane = lane_id();
+    bool over = false;
+    if (__popc(cm) == 1) {
+        const u32 k = __ffs(cm) - 1;
+        const u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
+        bytes += 8u + 4ull * (hi - lo);
+        __syncwarp();
+        if (lane == 0) {
+            ws->cadj |= bit;
+            ws->clo[d] = lo;
+            ws->clen[d] = hi - lo;
+        }
+        __syncwarp();
+    } else {
+        u32 best = 0, blo = 0, blen = 0xFFFFFFFFu;
+        u64 by = 0;
+        for (u32 m = cm; m; m &= m - 1) {
+            const u32 k = __ffs(m) - 1;
+            const u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
+            by += 8u + 4ull * (hi - lo);
+            if (hi - lo < blen) blen = hi - lo, blo = lo, best = k;
+        }
+        bytes += by;
+        u32* out = slot_list(ws, d);
+        const u32 rest = cm & ~(1u << best);
+        u32 n = 0;
+        for (u32 j = 0; j < blen; j += 32) {
+            bool ok = j + lane < blen;
+            const u32 x = ok ? __ldg(q.adj + blo + j + lane) : 0u;
+            for (u32 m = rest; m && ok; m &= m - 1) {
+                const u32 k = __ffs(m) - 1;
+                ok = contains_u32(q.adj, row_lo(q, d, k, ws->pos), row_hi(q, d, k, ws->pos), x);
+            }
+            const u32 bal = __ballot_sync(FULL_MASK, ok);
+            const u32 c = __popc(bal);
+            if (n + c > CACHE_CAP) {
+                over = true;
+                break;
+            }
+            if (ok) out[n + __popc(bal & ((1u << lane) - 1u))] = x;
+            n += c;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            ws->cadj &= ~bit;
+            ws->clen[d] = over ? 0u : n;
+        }
+        __syncwarp();
+    }
+    if (!over && ((q.bm_depths >> d) & 1u)) set_bits(q, ws, d);
+    if (lane == 0) {
+        if (over)
+            ws->cover |= bit;
+        else
+            ws->cvalid |= bit;
+    }
+    __syncwarp();
+    return !over;
+}
+
+// Whether to walk R (length r) and test S through its bitmap rather than
+// walk the shorter side and binary-search the other.
+__device__ __forceinline__ bool walk_r_with_bitmap(const WarpStack* ws, u32 d, u32 r, u32 s) {
+    return ((ws->cbits >> d) & 1u) && r <= 2u * s + 32u;
+}
+
+// Sets up depth d for the current prefix: cached mode when the depth's cache
+// is usable, else the shortest backward-neighbour row drives and the others
+// are tested. Adds the algorithmic bytes of the arrays intersected; returns
+// the driver length.
+__device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws, u64& bytes) {
+    u32 flg = 0, best = 0, dlo = 0, dhi = 0, olo = 0, ohi = 0;
+    if (ensure_cache(q, d, ws, bytes)) {
+        const u32 s = ws->clen[d];
+        const u32 k = q.crow[d];
+        flg = LV_CACHED | LV_DRV_CACHE;
+        dhi = s;
+        bytes += 4ull * s;
+        if (k != NO_ROW) {
+            const u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
+            bytes += 8u + 4ull * (hi - lo);
+            if (walk_r_with_bitmap(ws, d, hi - lo, s)) {
+                flg = LV_CACHED | LV_OTHER | LV_OTHER_BM;
+                best = k, dlo = lo, dhi = hi;
+            } else if (hi - lo < s) {
+                flg = LV_CACHED | LV_OTHER;
+                best = k, dlo = lo, dhi = hi, olo = 0, ohi = s;
+            } else {
+                flg |= LV_OTHER;
+                olo = lo, ohi = hi;
+            }
+        }
+    } else {
+        const u32 nb = q.nbn[d];
+        u32 blen = 0xFFFFFFFFu;
+        u64 by = 0;
+        for (u32 k = 0; k < nb; ++k) {
+            u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
+            by += 8u + 4ull * (hi - lo);
+            if (hi - lo < blen) blen = hi - lo, best = k, dlo = lo, dhi = hi;
+        }
+        bytes += by;
+    }
+    __syncwarp();
+    if (lane_id() == 0) {
+        ws->flg[d] = flg;
         ws->drv[d] = best;
-        ws->cur[d] = bs;
-        ws->end[d] = bs + blen;
+        ws->cur[d] = dlo;
+        ws->end[d] = dhi;
+        ws->olo[d] = olo;
+        ws->ohi[d] = ohi;
         ws->cn[d] = 0;
         ws->ci[d] = 0;
     }
     __syncwarp();
-    return blen;
+    return dhi - dlo;
+}
+
+// Element idx of depth d's driver array (d >= 1).
+__device__ __forceinline__ u32 drv_elem(const QState& q, const WarpStack* ws, u32 d, u32 idx) {
+    return (ws->flg[d] & LV_DRV_CACHE) ? cache_list(q, ws, d)[idx] : q.adj[idx];
+}
+
+// True if position x lies in depth d's driver range [lo, hi).
+__device__ __forceinline__ bool drv_contains(const QState& q, const WarpStack* ws, u32 d, u32 lo, u32 hi, u32 x) {
+    return (ws->flg[d] & LV_DRV_CACHE) ? contains_rw(cache_list(q, ws, d), lo, hi, x)
+                                       : contains_u32(q.adj, lo, hi, x);
 }
 
 // Position of data vertex v (same label as query vertex u) among the sorted
@@ -143,14 +355,28 @@ __device__ __forceinline__ void cap_reached(QState& q) {
 }
 
 // One lane's candidate test at depth d for driver element p (a position in
-// C(u_d)): member of every other row and not a data vertex already used by a
-// same-label earlier depth.
+// C(u_d)): member of every other array of the level and not a data vertex
+// already used by a same-label earlier depth.
 __device__ __forceinline__ bool accept(const QState& q, u32 d, u32 p, const WarpStack* ws, const u32* list_d) {
-    const u32 nb = q.nbn[d], drv = ws->drv[d];
-    for (u32 k = 0; k < nb; ++k) {
-        if (k == drv) continue;
-        u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
-        if (!contains_u32(q.adj, lo, hi, p)) return false;
+    const u32 f = ws->flg[d];
+    if (f & LV_CACHED) {
+        if (f & LV_OTHER) {
+            bool in;
+            if (f & LV_OTHER_BM)
+                in = bm_test(slot_bm(ws, d), p);
+            else if (f & LV_DRV_CACHE)
+                in = contains_u32(q.adj, ws->olo[d], ws->ohi[d], p);
+            else
+                in = contains_rw(cache_list(q, ws, d), ws->olo[d], ws->ohi[d], p);
+            if (!in) return false;
+        }
+    } else {
+        const u32 nb = q.nbn[d], drv = ws->drv[d];
+        for (u32 k = 0; k < nb; ++k) {
+            if (k == drv) continue;
+            u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
+            if (!contains_u32(q.adj, lo, hi, p)) return false;
+        }
     }
     u32 m = q.same_mask[d];
     if (m) {
@@ -176,36 +402,27 @@ __device__ u64 count_last(const QState& q, u32 d, WarpStack* ws, u64& bytes, u64
     const u32 lane = lane_id();
     const u32 u = q.order[d];
     const u32* list_d = q.list[u];
-    const u32 nb = q.nbn[d];
-    u32 best = 0, blen = 0xFFFFFFFFu, bs = 0;
-    u64 by = 0;
-    for (u32 k = 0; k < nb; ++k) {
-        u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
-        u32 len = hi - lo;
-        by += 8u + 4ull * len;
-        if (len < blen) blen = len, best = k, bs = lo;
-    }
-    bytes += by;
-    calls += blen;
-    if (blen == 0) return 0;
-    const u32 same = q.same_mask[d];
-    if (nb == 1) {
-        if (!same) return blen;
-        // Subtract used same-label vertices whose position is in the row.
+    const u32 len = setup_level(q, d, ws, bytes);
+    calls += len;
+    if (len == 0) return 0;
+    const u32 f = ws->flg[d];
+    const u32 lo = ws->cur[d], hi = ws->end[d];
+    const bool single = (f & LV_CACHED) ? !(f & LV_OTHER) : q.nbn[d] == 1;
+    if (single) {
+        // every driver entry is a candidate: subtract the used same-label
+        // vertices whose position is in the range
+        const u32 same = q.same_mask[d];
         u32 hit = 0;
         if ((same >> lane) & 1u) {
-            u32 x = cand_pos(q, u, ws->vid[lane]);
-            hit = (x != 0xFFFFFFFFu && contains_u32(q.adj, bs, bs + blen, x)) ? 1u : 0u;
+            const u32 x = cand_pos(q, u, ws->vid[lane]);
+            hit = (x != 0xFFFFFFFFu && drv_contains(q, ws, d, lo, hi, x)) ? 1u : 0u;
         }
-        return blen - __popc(__ballot_sync(FULL_MASK, hit));
+        return len - __popc(__ballot_sync(FULL_MASK, hit));
     }
-    __syncwarp();
-    if (lane == 0) ws->drv[d] = best;
-    __syncwarp();
     u64 c = 0;
-    for (u32 j = 0; j < blen; j += 32) {
-        const bool valid = j + lane < blen;
-        const u32 p = valid ? q.adj[bs + j + lane] : 0u;
+    for (u32 j = 0; j < len; j += 32) {
+        const bool valid = j + lane < len;
+        const u32 p = valid ? drv_elem(q, ws, d, lo + j + lane) : 0u;
         c += __popc(__ballot_sync(FULL_MASK, chunk_accept(q, d, p, valid, ws, list_d)));
     }
     return c;
@@ -226,7 +443,7 @@ __device__ u64 emit_last(QState& q, const DevGraph& g, u32 d, WarpStack* ws, u64
         bool ok = false;
         u32 p = 0;
         if (j + lane < blen) {
-            p = q.adj[bs + j + lane];
+            p = drv_elem(q, ws, d, bs + j + lane);
             ok = accept(q, d, p, ws, list_d);
         }
         u32 bal = __ballot_sync(FULL_MASK, ok);
@@ -248,19 +465,73 @@ __device__ u64 emit_last(QState& q, const DevGraph& g, u32 d, WarpStack* ws, u64
     return c;
 }
 
-// Last-depth count for one lane: the lane's own candidate p (data vertex v)
-// sits at depth dl - 1, the rest of the prefix is shared in ws. Counts the
-// positions in the intersection of the backward-neighbour rows of depth dl
-// whose data vertex differs from every same-label vertex of the embedding.
-// An intersection whose shortest row is longer than LONG_ROW is not walked by
-// the lane: it sets *defer and the warp counts it cooperatively afterwards
-// (warp_last_count), so one hub row does not stall 31 idle lanes.
-constexpr u32 LONG_ROW = 24;
+// Last-depth counts of the fused last two depths. The lane's own candidate
+// p (data vertex v) sits at depth dl - 1, the rest of the prefix is shared
+// in ws. A count is the number of positions in the intersection of the
+// backward-neighbour rows of depth dl whose data vertex differs from every
+// same-label vertex of the embedding. With `cached`, depth dl's cache S
+// (warp-shared, valid for the prefix) stands for the rows of depths
+// <= dl - 2, and only the lane's own row R (when p's depth is a backward
+// neighbour) is intersected with it: R walked against S's bitmap, or the
+// shorter side binary-searched in the other. A walk longer than LONG_ROW
+// (LONG_BM_ROW for bitmap walks) is not done by the lane: it sets *defer and
+// the warp counts it cooperatively afterwards (warp_last_count), so one hub
+// row does not stall 31 idle lanes.
 
-__device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const WarpStack* ws, u64& bytes, u64& calls,
-                               bool* defer) {
+// Used same-label vertices (the lane's own v at depth dl - 1, the rest from
+// ws) whose position lies in S of dl and, when has_row, in R = adj[lo, hi).
+__device__ __forceinline__ u32 cached_exclusions(const QState& q, u32 dl, u32 v, const WarpStack* ws, bool has_row,
+                                                 u32 lo, u32 hi) {
+    const u32 u = q.order[dl];
+    const u32 dp = dl - 1;
+    u32 c = 0;
+    for (u32 m = q.same_mask[dl]; m; m &= m - 1) {
+        const u32 j = __ffs(m) - 1;
+        const u32 x = cand_pos(q, u, j == dp ? v : ws->vid[j]);
+        if (x != 0xFFFFFFFFu && in_cache(q, ws, dl, x) && (!has_row || contains_u32(q.adj, lo, hi, x))) ++c;
+    }
+    return c;
+}
+
+__device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 v, const WarpStack* ws, u64& bytes,
+                               u64& calls, bool* defer) {
     const u32 nb = q.nbn[dl];
     const u32 dp = dl - 1;
+    if (cached) {
+        const u32 s = ws->clen[dl];
+        const u32 k = q.crow[dl];
+        if (k == NO_ROW) {
+            calls += s;
+            return s - cached_exclusions(q, dl, v, ws, false, 0, 0);
+        }
+        const u32 base = q.bn_tab[dl][k] + p;
+        const u32 lo = q.P[base], hi = q.P[base + 1], r = hi - lo;
+        bytes += 8u + 4ull * r + 4ull * s;
+        if (s == 0 || r == 0) return 0;
+        u64 c = 0;
+        if (walk_r_with_bitmap(ws, dl, r, s)) {
+            calls += r;
+            if (r > LONG_BM_ROW) {
+                *defer = true;
+                return 0;
+            }
+            const u32* bm = slot_bm(ws, dl);
+            for (u32 e = lo; e < hi; ++e) c += bm_test(bm, __ldg(q.adj + e));
+        } else {
+            calls += min(s, r);
+            if (min(s, r) > LONG_ROW) {
+                *defer = true;
+                return 0;
+            }
+            const u32* S = cache_list(q, ws, dl);
+            if (r <= s) {
+                for (u32 e = lo; e < hi; ++e) c += contains_rw(S, 0, s, __ldg(q.adj + e));
+            } else {
+                for (u32 i = 0; i < s; ++i) c += contains_u32(q.adj, lo, hi, S[i]);
+            }
+        }
+        return c - cached_exclusions(q, dl, v, ws, true, lo, hi);
+    }
     u32 blo = 0, bhi = 0, blen = 0xFFFFFFFFu, bk = 0;
     u64 by = 0;
     for (u32 k = 0; k < nb; ++k) {
@@ -316,13 +587,44 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, u32 p, u32 v, const Warp
 }
 
 // Warp-cooperative form of lane_last_count for one (p, v) (warp-uniform):
-// the shortest row is walked 32 entries at a time, each lane binary-searching
-// its entry in the other rows. Rows and bytes were counted by the lane that
+// the walked side is taken 32 entries at a time, each lane testing its entry
+// against the other arrays. Rows and bytes were counted by the lane that
 // deferred it.
-__device__ u64 warp_last_count(const QState& q, u32 dl, u32 p, u32 v, const WarpStack* ws) {
+__device__ u64 warp_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 v, const WarpStack* ws) {
     const u32 lane = lane_id();
     const u32 nb = q.nbn[dl];
     const u32 dp = dl - 1;
+    if (cached) {
+        // deferred only with a row at depth dl - 1
+        const u32 s = ws->clen[dl];
+        const u32 base = q.bn_tab[dl][q.crow[dl]] + p;
+        const u32 lo = q.P[base], hi = q.P[base + 1], r = hi - lo;
+        u64 c = 0;
+        if (walk_r_with_bitmap(ws, dl, r, s)) {
+            const u32* bm = slot_bm(ws, dl);
+            for (u32 e0 = lo; e0 < hi; e0 += 32) {
+                const u32 e = e0 + lane;
+                const bool ok = e < hi && bm_test(bm, __ldg(q.adj + e));
+                c += __popc(__ballot_sync(FULL_MASK, ok));
+            }
+        } else {
+            const u32* S = cache_list(q, ws, dl);
+            if (r <= s) {
+                for (u32 e0 = lo; e0 < hi; e0 += 32) {
+                    const u32 e = e0 + lane;
+                    const bool ok = e < hi && contains_rw(S, 0, s, __ldg(q.adj + e));
+                    c += __popc(__ballot_sync(FULL_MASK, ok));
+                }
+            } else {
+                for (u32 i0 = 0; i0 < s; i0 += 32) {
+                    const u32 i = i0 + lane;
+                    const bool ok = i < s && contains_u32(q.adj, lo, hi, S[i]);
+                    c += __popc(__ballot_sync(FULL_MASK, ok));
+                }
+            }
+        }
+        return c - cached_exclusions(q, dl, v, ws, true, lo, hi);
+    }
     u32 blo = 0, bhi = 0, blen = 0xFFFFFFFFu, bk = 0;
     for (u32 k = 0; k < nb; ++k) {
         const u32 bd = q.bn_depth[dl][k];
@@ -493,7 +795,9 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
             if (ws->end[dd] - ws->cur[dd] >= 64u) break;
         if (dd <= d) {
             u32 end = ws->end[dd];
-            bool done = try_donate_range(ctl, slots, KIND_RANGE, qi, dd, ws->cur[dd], end, ws->drv[dd], ws, 64u);
+            // drv word: bn index of the driver | level flags << 16
+            bool done = try_donate_range(ctl, slots, KIND_RANGE, qi, dd, ws->cur[dd], end,
+                                         ws->drv[dd] | (ws->flg[dd] << 16), ws, 64u);
             __syncwarp();
             if (done && lane == 0) ws->end[dd] = end;
             __syncwarp();
@@ -557,19 +861,21 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
                 u64 c = 0;
                 bool defer = false;
                 const u32* list_d = q.list[q.order[d]];
+                // the last depth's cache depends on depths <= d - 1 only
+                const bool cached = ensure_cache(q, d + 1, ws, bytes);
                 const bool valid = idx < end;
-                const u32 p = valid ? (d == 0 ? idx : q.adj[idx]) : 0u;
+                const u32 p = valid ? (d == 0 ? idx : drv_elem(q, ws, d, idx)) : 0u;
                 const bool ok = d == 0 ? valid : chunk_accept(q, d, p, valid, ws, list_d);
                 const u32 v = ok ? list_d[p] : 0u;
-                if (ok) c = lane_last_count(q, d + 1, p, v, ws, bytes_l, calls_l, &defer);
+                if (ok) c = lane_last_count(q, d + 1, cached, p, v, ws, bytes_l, calls_l, &defer);
                 count += warp_sum64(c);
                 // long intersections deferred by their lanes: whole warp each
                 u32 dm = __ballot_sync(FULL_MASK, defer);
                 while (dm) {
                     const u32 src = __ffs(dm) - 1;
                     dm &= dm - 1;
-                    count += warp_last_count(q, d + 1, __shfl_sync(FULL_MASK, p, src), __shfl_sync(FULL_MASK, v, src),
-                                             ws);
+                    count += warp_last_count(q, d + 1, cached, __shfl_sync(FULL_MASK, p, src),
+                                             __shfl_sync(FULL_MASK, v, src), ws);
                 }
                 calls += min(32u, end - cur);
                 __syncwarp();
@@ -592,6 +898,9 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
                 ws->ci[d] += 1;
                 ws->pos[d] = p;
                 ws->vid[d] = q.list[q.order[d]][p];
+                const u32 inv = q.cinval[d];  // caches that depend on depth d
+                ws->cvalid &= ~inv;
+                ws->cover &= ~inv;
             }
             __syncwarp();
             if (d + 2 == n) {
@@ -604,7 +913,7 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
             const u32 cur = ws->cur[d], end = ws->end[d];
             const u32 idx = cur + lane;
             const bool valid = idx < end;
-            const u32 p = valid ? (d == 0 ? idx : q.adj[idx]) : 0u;
+            const u32 p = valid ? (d == 0 ? idx : drv_elem(q, ws, d, idx)) : 0u;
             const bool ok = d == 0 ? valid : chunk_accept(q, d, p, valid, ws, q.list[q.order[d]]);
             u32 bal = __ballot_sync(FULL_MASK, ok);
             if (ok) ws->chunk[d][__popc(bal & ((1u << lane) - 1u))] = p;
@@ -650,6 +959,7 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
     if (warp_ld_volatile_u32(&q.stop)) return;
     u64 count = 0, bytes = 0, calls = 0;
     u32 iter = 0;
+    // caches start empty (release_caches ran at the end of the last task)
     if (n == 1) {  // single-vertex query: every root candidate is an embedding
         count = t.e - t.b;
         calls = count;
@@ -678,7 +988,7 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
             else
                 hi = mid;
         }
-        u32 r = lo;
+        u32 r = lo, last_r = 0xFFFFFFFFu;
         u32 end = t.e;
         for (u32 e = t.b; e < end; ++e) {
             while (q.P[base + r + 1] <= e) ++r;
@@ -692,13 +1002,18 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
                 ws->vid[0] = v0;
                 ws->pos[1] = c;
                 ws->vid[1] = v1;
+                const u32 inv = q.cinval[r == last_r ? 1 : 0];
+                ws->cvalid &= ~inv;
+                ws->cover &= ~inv;
             }
+            last_r = r;
             __syncwarp();
             // edge pools are built for queries of four or more vertices
             setup_level(q, 2, ws, bytes);
             if (!dfs(g, q, t.qi, 2, ws, ctl, slots, emit, count, bytes, calls, iter)) break;
             if (e + 2 < end) try_donate_range(ctl, slots, KIND_EDGES, t.qi, 0, e + 1, end, 0, ws, 2u);
         }
+        release_caches(q, ws);
         publish(q, count, bytes, calls);
         return;
     }
@@ -713,11 +1028,37 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
         if (t.kind == KIND_FULL) {
             setup_level(q, d0, ws, bytes);
         } else {
+            // a donated driver range: rebuild the level the donor had (its
+            // cache is a function of the prefix, so the range indexes the
+            // same array here)
+            const u32 flg = t.drv >> 16, k = t.drv & 0xFFFFu;
+            u32 olo = 0, ohi = 0;
+            if (flg & LV_CACHED) {
+                // the donor's flags need what the donor had: the cache, and
+                // its bitmap when S is tested through it
+                if (!ensure_cache(q, d0, ws, bytes) || ((flg & LV_OTHER_BM) && !((ws->cbits >> d0) & 1u))) {
+                    if (lane == 0) atomicExch(&ctl->error, 1u);
+                    release_caches(q, ws);
+                    publish(q, count, bytes, calls);
+                    return;
+                }
+                if ((flg & LV_OTHER) && !(flg & LV_OTHER_BM)) {
+                    if (flg & LV_DRV_CACHE) {
+                        olo = row_lo(q, d0, q.crow[d0], ws->pos);
+                        ohi = row_hi(q, d0, q.crow[d0], ws->pos);
+                    } else {
+                        ohi = ws->clen[d0];
+                    }
+                }
+            }
             __syncwarp();
             if (lane == 0) {
+                ws->flg[d0] = flg;
                 ws->cur[d0] = t.b;
                 ws->end[d0] = t.e;
-                ws->drv[d0] = t.drv;
+                ws->drv[d0] = k;
+                ws->olo[d0] = olo;
+                ws->ohi[d0] = ohi;
                 ws->cn[d0] = 0;
                 ws->ci[d0] = 0;
             }
@@ -725,6 +1066,7 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
         }
         dfs(g, q, t.qi, d0, ws, ctl, slots, emit, count, bytes, calls, iter);
     }
+    release_caches(q, ws);
     publish(q, count, bytes, calls);
 }
 
@@ -776,10 +1118,19 @@ __device__ bool take_initial(EnumCtl* ctl, const u32* grab_prefix, const PoolInf
 
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 4) enum_kernel(DevGraph g, QState* qs, EnumCtl* ctl,
                                                                     Slot* slots, const u32* grab_prefix,
-                                                                    const PoolInfo* pools, int emit) {
+                                                                    const PoolInfo* pools, int emit, u32* cache) {
     __shared__ WarpStack stacks[WARPS_PER_BLOCK];
     WarpStack* ws = &stacks[threadIdx.x >> 5];
     const u32 lane = lane_id();
+    if (lane == 0) {
+        const size_t warp = (size_t)blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5);
+        ws->cbuf = cache ? cache + warp * (PSM_MAXQ * SLOT_WORDS) : nullptr;
+        ws->cvalid = 0;
+        ws->cover = 0;
+        ws->cbits = 0;
+        ws->cadj = 0;
+    }
+    __syncwarp();
     TaskHdr t;
     bool hungry = false;
     u64 spins = 0, ntasks = 0, npolls = 0;
@@ -920,12 +1271,17 @@ cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStre
 
 size_t psm_enum_scratch_bytes() { return align16(sizeof(EnumCtl)) + sizeof(Slot) * QCAP + 64; }
 
+// Per-warp prefix-intersection caches of a launch of `blocks` blocks.
+size_t psm_enum_cache_bytes(int blocks) {
+    return (size_t)blocks * WARPS_PER_BLOCK * PSM_MAXQ * SLOT_WORDS * sizeof(u32);
+}
+
 // Per-query scratch of the enumeration: grab prefix (nq + 1 words) and pool
 // descriptors.
 size_t psm_enum_query_bytes(u32 nq) { return align16(sizeof(u32) * (nq + 1)) + sizeof(PoolInfo) * nq; }
 
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
-                            int emit, int blocks, cudaStream_t st) {
+                            int emit, int blocks, u32* cache, cudaStream_t st) {
     EnumCtl* ctl = (EnumCtl*)scratch;
     Slot* slots = (Slot*)((char*)scratch + align16(sizeof(EnumCtl)));
     u32* grab_prefix = (u32*)query_scratch;
@@ -934,7 +1290,7 @@ cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch
                                          (u32)blocks * WARPS_PER_BLOCK, budget_ns);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    enum_kernel<<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, grab_prefix, pools, emit);
+    enum_kernel<<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, grab_prefix, pools, emit, cache);
     return cudaGetLastError();
 }
 

@@ -56,8 +56,11 @@ cudaError_t psm_launch_prep_cluster(const DevGraph& g, QState* qs, DevArena* are
                                     cudaStream_t st);
 size_t psm_enum_scratch_bytes();
 size_t psm_enum_query_bytes(u32 nq);
+size_t psm_enum_cache_bytes(int blocks);
+// cache: psm_enum_cache_bytes(blocks) of device memory for the per-warp
+// prefix-intersection caches, or null to run without them.
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
-                            int emit, int blocks, cudaStream_t st);
+                            int emit, int blocks, u32* cache, cudaStream_t st);
 cudaError_t psm_enum_max_blocks(int* blocks);
 cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st);
 cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st);

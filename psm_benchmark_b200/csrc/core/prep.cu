@@ -891,11 +891,37 @@ __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
         const u32 lb = __shfl_sync(FULL_MASK, lab, b);
         if (b < lane && lb == lab) same |= 1u << b;
     }
+    // prefix-intersection cache plan (the bn rows of this lane's depth are in
+    // bn_depth[lane][0, k), written by this lane above)
+    u32 cm = 0, crow = 0xFFFFFFFFu, cdep = 0;
+    for (u32 j = 0; j < k; ++j) {
+        const u32 bd = q.bn_depth[lane][j];
+        if (bd + 2 <= lane) {
+            cm |= 1u << j;
+            cdep = max(cdep, bd);
+        } else {
+            crow = j;  // bd == lane - 1
+        }
+    }
+    const bool bm_ok = act && q.cnt[u] <= PSM_CACHE_BM_BITS;
+    const u32 bm_depths = __ballot_sync(FULL_MASK, bm_ok);
+    // one shallow row is worth caching only as a bitmap tested against the
+    // depth-(d-1) row
+    if (__popc(cm) < 2 && !(__popc(cm) == 1 && crow != 0xFFFFFFFFu && bm_ok)) cm = 0;
+    u32 inval = 0;
+    for (u32 x = 0; x < n; ++x) {
+        const u32 bal = __ballot_sync(FULL_MASK, act && cm != 0 && cdep >= x);
+        if (lane == x) inval = bal;
+    }
     if (act) {
         q.nbn[lane] = k;
         q.same_mask[lane] = same;
         q.cbase[lane] = bucket_base(g, d->label[lane]);
+        q.cmask[lane] = cm;
+        q.crow[lane] = crow;
+        q.cinval[lane] = inval;
     }
+    if (lane == 0) q.bm_depths = bm_depths;
     // memory cost: candidates of every vertex, both tables of every edge
     u64 mem = 0;
     if (act) {

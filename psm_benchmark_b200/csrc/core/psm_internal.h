@@ -24,6 +24,7 @@
 #define PSM_PLAN_WORDS 4096  // CFL order plan blob capacity (u32 words)
 #define PSM_TRACE_STEPS 256  // preparation steps recorded when tracing (+1 start stamp)
 #define HYBRID_REQUEST 0xFFFFFFFFu  // QState.step_cursor on entry: use the hybrid grid driver
+#define PSM_CACHE_BM_BITS 32768u    // candidate positions covered by an enumerator cache bitmap
 
 typedef uint32_t u32;
 typedef uint64_t u64;
@@ -139,6 +140,20 @@ struct QState {
     u32 bn_tab[PSM_MAXQ][PSM_MAXQ - 1];   // row base into P for table T[bn][u_d]
     u32 same_mask[PSM_MAXQ];              // earlier depths with the same label
     u32 cbase[PSM_MAXQ];                  // first internal id of the bucket of u (by query vertex)
+    // Prefix-intersection cache plan (by depth d): cmask[d] = backward
+    // neighbours k (bits over bn index) whose depth is <= d - 2, when there are
+    // at least two of them, or one of them together with a backward neighbour
+    // at depth d - 1 and a bitmap-sized candidate set (else 0). Their rows'
+    // intersection depends only on the prefix up to cdep[d] = the deepest of
+    // them, so the enumerator keeps it per warp (sorted list, plus a bitmap
+    // over candidate positions when bm_depths has bit d) and reuses it for
+    // every node below that prefix. crow[d] = bn index of the backward
+    // neighbour at depth d - 1 (0xFFFFFFFF if none). cinval[x] = depths whose
+    // cache is invalidated when depth x changes (cmask[d] != 0, cdep[d] >= x).
+    u32 cmask[PSM_MAXQ];
+    u32 crow[PSM_MAXQ];
+    u32 cinval[PSM_MAXQ];
+    u32 bm_depths;                        // depths with |C(u_d)| <= PSM_CACHE_BM_BITS
     u32 root_cnt;
     // results
     u64 count;
