@@ -120,6 +120,7 @@ struct WarpStack {
     u32 ohi[PSM_MAXQ];
     u32 clen[PSM_MAXQ];
     u32 clo[PSM_MAXQ];
+    u32 csum[PSM_MAXQ];  // total length of the rows behind S (algorithmic bytes)
     u32 chunk[PSM_MAXQ][32];
 };
 
@@ -216,24 +217,22 @@ __device__ bool ensure_cache(const QState& q, u32 d, WarpStack* ws, u64& bytes) 
     if (__popc(cm) == 1) {
         const u32 k = __ffs(cm) - 1;
         const u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
-        bytes += 8u + 4ull * (hi - lo);
         __syncwarp();
         if (lane == 0) {
             ws->cadj |= bit;
             ws->clo[d] = lo;
             ws->clen[d] = hi - lo;
+            ws->csum[d] = hi - lo;
         }
         __syncwarp();
     } else {
-        u32 best = 0, blo = 0, blen = 0xFFFFFFFFu;
-        u64 by = 0;
+        u32 best = 0, blo = 0, blen = 0xFFFFFFFFu, tot = 0;
         for (u32 m = cm; m; m &= m - 1) {
             const u32 k = __ffs(m) - 1;
             const u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
-            by += 8u + 4ull * (hi - lo);
+            tot += hi - lo;
             if (hi - lo < blen) blen = hi - lo, blo = lo, best = k;
         }
-        bytes += by;
         u32* out = slot_list(ws, d);
         const u32 rest = cm & ~(1u << best);
         u32 n = 0;
@@ -257,6 +256,7 @@ __device__ bool ensure_cache(const QState& q, u32 d, WarpStack* ws, u64& bytes) 
         if (lane == 0) {
             ws->cadj &= ~bit;
             ws->clen[d] = over ? 0u : n;
+            ws->csum[d] = tot;
         }
         __syncwarp();
     }
@@ -279,7 +279,9 @@ __device__ __forceinline__ bool walk_r_with_bitmap(const WarpStack* ws, u32 d, u
 
 // Sets up depth d for the current prefix: cached mode when the depth's cache
 // is usable, else the shortest backward-neighbour row drives and the others
-// are tested. Adds the algorithmic bytes of the arrays intersected; returns
+// are tested. Adds the algorithmic bytes of the level -- those of the
+// reference's intersection of all backward-neighbour rows (8 B of offsets +
+// 4 B per entry each), whether or not a cache saved reading them; returns
 // the driver length.
 __device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws, u64& bytes) {
     u32 flg = 0, best = 0, dlo = 0, dhi = 0, olo = 0, ohi = 0;
@@ -288,10 +290,10 @@ __device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws
         const u32 k = q.crow[d];
         flg = LV_CACHED | LV_DRV_CACHE;
         dhi = s;
-        bytes += 4ull * s;
+        bytes += 8ull * q.nbn[d] + 4ull * ws->csum[d];
         if (k != NO_ROW) {
             const u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
-            bytes += 8u + 4ull * (hi - lo);
+            bytes += 4ull * (hi - lo);
             if (walk_r_with_bitmap(ws, d, hi - lo, s)) {
                 flg = LV_CACHED | LV_OTHER | LV_OTHER_BM;
                 best = k, dlo = lo, dhi = hi;
@@ -500,13 +502,14 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
     if (cached) {
         const u32 s = ws->clen[dl];
         const u32 k = q.crow[dl];
+        bytes += 8ull * nb + 4ull * ws->csum[dl];
         if (k == NO_ROW) {
             calls += s;
             return s - cached_exclusions(q, dl, v, ws, false, 0, 0);
         }
         const u32 base = q.bn_tab[dl][k] + p;
         const u32 lo = q.P[base], hi = q.P[base + 1], r = hi - lo;
-        bytes += 8u + 4ull * r + 4ull * s;
+        bytes += 4ull * r;
         if (s == 0 || r == 0) return 0;
         u64 c = 0;
         if (walk_r_with_bitmap(ws, dl, r, s)) {
@@ -1196,6 +1199,8 @@ __global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, 
                     pi.kind = KIND_EDGES;
                     pi.first = q.P[tb];
                     pi.units = q.P[tb + q.root_cnt] - pi.first;
+                    // depth 1 reads the first table's row of every root
+                    atomicAdd((unsigned long long*)&qs[i].alg_bytes, 8ull * q.root_cnt + 4ull * pi.units);
                 } else {
                     pi.kind = KIND_RANGE;
                     pi.first = 0;

@@ -5,6 +5,8 @@ embedding counts must be identical (bit-exact integer results) to what the
 reference computes: its recorded HPRD counts and the fixtures dumped from the
 reference's own code (tests/golden), plus the oracle restatement on extra
 cases."""
+import os
+
 import numpy as np
 import pytest
 
@@ -115,3 +117,38 @@ def test_cap_is_exact(engine):
     assert full > 1000
     for cap in (1, 7, 999, full - 1, full, full + 5):
         assert api.match(engine, dg, star, "CFL_CFL_EXPLORE", cap=cap).count == min(full, cap)
+
+
+def test_algorithmic_bytes_match_oracle(engine):
+    """The enumerator's algorithmic bytes (the input volume of the
+    reference's intersections: 8 B of row offsets + 4 B per entry of every
+    backward-neighbour row, for every extended partial embedding) equal the
+    oracle's instrumented count, with and without the enumerator's caches."""
+    g, qs, counts = gd.hprd()
+    og = OracleGraph(g)
+    dg = api.DataGraph.from_graph(g)
+    os.environ["PSM_ENUM_CACHE"] = "0"
+    try:
+        plain_engine = api.Engine(arena_bytes=1 << 30)
+    finally:
+        del os.environ["PSM_ENUM_CACHE"]
+    try:
+        for q in qs:
+            for f, o, m in (("CFL", "CFL", "CFL_CFL_EXPLORE"), ("GQL", "GQL", "GQL_GQL_GQL")):
+                ref = og.run(q, f, o, want_tables=False)
+                for e in (engine, plain_engine):
+                    got = api.match(e, dg, q, m)
+                    assert got.count == ref.count
+                    assert got.alg_bytes == int(ref.depth_bytes.sum()), (f, o)
+    finally:
+        plain_engine.close()
+    syn = gd.synthetic_graph("plain_small")
+    og = OracleGraph(syn)
+    dg = api.DataGraph.from_graph(syn)
+    case = dict(gd.synthetic_cases())["plain_small"]
+    for entry in case["queries"][:12]:
+        q = gd.query_from_rec(entry["query"])
+        ref = og.run(q, "GQL", "GQL", want_tables=False)
+        got = api.match(engine, dg, q, "GQL_GQL_GQL")
+        assert got.count == ref.count
+        assert got.alg_bytes == int(ref.depth_bytes.sum())
