@@ -112,7 +112,11 @@ def dist_setup():
 
 def make_workload(args):
     from psm_benchmark_b200 import gen
-    return gen.plain_rmat(num_queries=args.queries, scale=args.scale)
+    w = gen.plain_rmat(num_queries=args.queries, scale=args.scale)
+    if args.only:
+        # a subset of the workload's queries (profiling of single launches)
+        w.queries = [w.queries[int(i)] for i in args.only.split(",")]
+    return w
 
 
 # --------------------------------------------------------------- reference --
@@ -265,6 +269,7 @@ def ours_arm(args, world, rank, local):
     dev_ms = 0.0
     enum_ms = 0.0
     alg = 0
+    lat = []
     h2d = d2h = 0
     counts = None
     t0 = time.perf_counter()
@@ -273,6 +278,7 @@ def ours_arm(args, world, rank, local):
         torch.cuda.synchronize()
         res = step()
         dev_ms += sum(r.prep_ms + r.enum_ms for r in res)
+        lat += [r.prep_ms + r.enum_ms for r in res]
         enum_ms += sum(r.enum_ms for r in res)
         alg += sum(r.alg_bytes for r in res)
         h2d += sum(r.h2d_bytes for r in res)
@@ -302,6 +308,9 @@ def ours_arm(args, world, rank, local):
                        "cap": w.cap, "parallelism": f"replicas x{world}",
                        "l2": "flushed (256 MiB write) before every step; 72 MB graph L2-resident within a step"},
             "embeddings_per_s": world * sum(counts) * args.steps / (dev_ms / 1e3),
+            # per-query device latency of the plain path (preparation + enumeration)
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(max(lat))},
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
             # per plain-path query: prep, enum-init, enum, gather kernels + 2 memsets
@@ -313,17 +322,18 @@ def ours_arm(args, world, rank, local):
     # enumeration launch for the whole step (device time, CUDA events).
     bt = 0.0
     bres = None
-    for s in range(args.steps + 1):
+    for s in range(args.steps + 1 if args.batched else 0):
         flush_l2(flush)
         torch.cuda.synchronize()
         bres = api.match_batch(eng, dg, w.queries, w.method, cap=w.cap, time_limit=args.time_limit)
         if s > 0:
             bt += bres[0].prep_ms + bres[0].enum_ms
-    if [r.count for r in bres] != counts:
-        raise SystemExit("batched counts differ from the plain path")
-    bval = world * nq * args.steps / (bt / 1e3)
-    line["batched"] = {"value": bval, "unit": "queries/s", "ms_per_step": bt / args.steps,
-                       "speedup_vs_plain": bval / value, "launches_per_step": 5}
+    if bres is not None:
+        if [r.count for r in bres] != counts:
+            raise SystemExit("batched counts differ from the plain path")
+        bval = world * nq * args.steps / (bt / 1e3)
+        line["batched"] = {"value": bval, "unit": "queries/s", "ms_per_step": bt / args.steps,
+                           "speedup_vs_plain": bval / value, "launches_per_step": 4}
     if rank == 0 and args.cpu_baseline and ref_available():
         rr = ReferenceRunner(w)
         qeq, tot, runs = rr.sample(REF_THREADS, args.ref_budget)
@@ -353,6 +363,8 @@ def main():
     ap.add_argument("--arena-gb", type=int, default=8)
     ap.add_argument("--ref-budget", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-batched", dest="batched", action="store_false")
+    ap.add_argument("--only", default="", help="comma-separated query indices (profiling runs)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
