@@ -138,12 +138,96 @@ void psm_run_free(psm_run* run);
  * Writes min(total, cap) to *count (cap 0 = none). */
 int psm_run_recount_noalloc(psm_run* run, uint64_t cap, double time_limit_s, uint64_t* count, uint32_t* overtime);
 
+/* ---- decomposition + join path (replaces split_Q_test,
+ *      matching/StudyPerformance.cpp:100-1037: SplitGraph units
+ *      (utility/splitGraph/SplitGraph.cpp:23-36), per-unit enumeration into
+ *      PartialMatch relations (Args.cpp:162-166), JoinCollect::sequence_collect
+ *      (matching/JoinCollect.cpp:237-315) with NoPartitionHashJoin
+ *      (utility/hashjoin/hashjoin.cpp:337-779)) ---- */
+#define PSM_MAX_UNITS 32
+typedef struct psm_join_result {
+    uint64_t count;                      /* #Embeddings = rows of the last join (min with the cap) */
+    uint32_t units;                      /* decomposition units */
+    uint32_t status;                     /* psm_status */
+    uint32_t unit_mask[PSM_MAX_UNITS];   /* query vertices of each unit (bit mask) */
+    uint64_t unit_rows[PSM_MAX_UNITS];   /* embeddings of each unit */
+    uint64_t join_rows[PSM_MAX_UNITS];   /* rows after joining units 0..k (join_rows[0] = unit_rows[0]) */
+    double prep_ms;                      /* device time: filter + tables + order of the whole query */
+    double enum_ms;                      /* device time: counting and emitting the units */
+    double join_ms;                      /* device time: the hash joins */
+    uint64_t work_bytes;                 /* device bytes of unit relations and join buffers */
+    uint64_t memory_bytes;               /* computeMemoryCostInBytes of the whole query */
+} psm_join_result;
+/* Filters the whole query and builds its tables (as the reference does in Q
+ * mode), splits it into connected units of at most max_unit_vertices
+ * vertices (every query edge in some unit), enumerates every unit on the
+ * query's candidates and tables, materialises the unit embeddings and joins
+ * them left-deep on their shared query vertices with device hash tables
+ * (load factor <= 0.5), keeping only injective rows; the last join is
+ * counted, not materialised. opt->cap applies to the final count. */
+int psm_match_join(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
+                   uint32_t max_unit_vertices, psm_join_result* res);
+/* The decomposition psm_match_join uses (host only): *num_units units,
+ * unit_masks[PSM_MAX_UNITS] their vertex sets. */
+int psm_query_decompose(const psm_query_desc* q, uint32_t max_unit_vertices, uint32_t* num_units,
+                        uint32_t* unit_masks);
+/* One hash join of host relations (replaces JoinCollect::concateTwoTabels,
+ * matching/JoinCollect.cpp:60-153): rows of r_cols / s_cols data vertex ids,
+ * column c of R holds query vertex r_vertex[c] (likewise S). Keys are the
+ * query vertices in both; R is the build side, S probes. An output row is
+ * S's columns then R's non-key columns (out_vertex / *out_cols describe
+ * them), kept iff no R non-key value occurs in the S row among columns of
+ * the same label (vertex_label[query vertex]; NULL = one label for all).
+ * out_rows == NULL counts only; otherwise out_capacity rows must suffice
+ * (else PSM_ERR_ARG with *out_n set to the count). */
+int psm_hash_join(psm_context* ctx, const uint32_t* r_rows, uint64_t r_n, uint32_t r_cols, const uint32_t* r_vertex,
+                  const uint32_t* s_rows, uint64_t s_n, uint32_t s_cols, const uint32_t* s_vertex,
+                  const uint32_t* vertex_label, uint32_t* out_rows, uint64_t out_capacity, uint32_t* out_vertex,
+                  uint32_t* out_cols, uint64_t* out_n);
 /* ---- batched path: many queries through one persistent preparation launch
  *      and one persistent enumeration launch (no counterpart in the
  *      reference, which runs queries one process at a time) ---- */
 int psm_match_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, uint32_t nq,
                     const psm_options* opt, psm_result* results);
 
+/* ---- serving: request loop with continuous batching over a resident graph
+ *      (no counterpart in the reference, which runs one query per process) ---- */
+typedef struct psm_server psm_server;
+typedef struct psm_server_config {
+    uint32_t lanes;             /* concurrent batches: each lane has its own stream, arena, enumerator */
+    uint32_t max_batch;         /* queries per batch */
+    uint64_t lane_arena_bytes;  /* device arena per lane; requests are admitted within it */
+    uint32_t full_gpu_lanes;    /* 1: every lane's launches may fill the whole GPU; 0: grids of 1/lanes */
+    uint32_t reserved;
+} psm_server_config;
+typedef struct psm_request_result {
+    uint64_t ticket;
+    uint64_t count;             /* #Embeddings = min(total, cap) */
+    uint32_t status;            /* psm_status of the request */
+    uint32_t overtime;
+    uint64_t submit_ns;         /* psm_server_clock_ns() stamps */
+    uint64_t start_ns;          /* its batch started */
+    uint64_t done_ns;           /* its batch finished */
+    uint32_t batch_size;        /* queries in its batch */
+    uint32_t lane;
+    double prep_ms;             /* device time of its batch's preparation */
+    double enum_ms;             /* device time of its batch's enumeration */
+} psm_request_result;
+/* Starts the lanes (threads) of a server for graph g (which must outlive it)
+ * with the method, cap and time limit of *opt. */
+int psm_server_create(int device, const psm_graph* g, const psm_options* opt, const psm_server_config* cfg,
+                      psm_server** out);
+/* Queues a copy of the query; *ticket identifies its result. */
+int psm_server_submit(psm_server* s, const psm_query_desc* q, uint64_t* ticket);
+/* Takes up to max finished results, waiting up to wait_s seconds for one. */
+int psm_server_poll(psm_server* s, psm_request_result* out, uint32_t max, uint32_t* n, double wait_s);
+/* Requests queued (not admitted) and running. */
+int psm_server_pending(psm_server* s, uint64_t* queued, uint64_t* running);
+/* The device memory a request is admitted with, and a lane's budget. */
+int psm_server_estimate(psm_server* s, const psm_query_desc* q, uint64_t* bytes, uint64_t* lane_budget);
+uint64_t psm_server_clock_ns(void);
+/* Finishes the running batches and stops; queued requests are dropped. */
+void psm_server_destroy(psm_server* s);
 #ifdef __cplusplus
 }
 #endif

@@ -210,3 +210,162 @@ class Run:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------- join path --
+
+@dataclass
+class JoinResult:
+    count: int
+    units: list            # vertex masks of the decomposition units
+    unit_rows: list        # embeddings of each unit
+    join_rows: list        # rows after joining units 0..k
+    prep_ms: float
+    enum_ms: float
+    join_ms: float
+    work_bytes: int
+    memory_bytes: int
+
+
+def match_join(engine: Engine, data: DataGraph, query: Graph, method: str = "CFL_CFL_EXPLORE",
+               max_unit_vertices: int = 12, cap: int = 0, time_limit: float = 60.0) -> JoinResult:
+    """Decomposition + hash-join path: the query is filtered and tabled
+    whole, split into connected units of at most max_unit_vertices vertices,
+    each unit's embeddings are materialised on the device and joined
+    left-deep on shared query vertices."""
+    qb = _QueryBuf(query)
+    opt = options(method, cap, time_limit)
+    r = N.JoinResult()
+    N.check(N.lib().psm_match_join(engine._h, data._h, C.byref(qb.desc), C.byref(opt), int(max_unit_vertices),
+                                   C.byref(r)))
+    u = r.units
+    return JoinResult(count=r.count, units=list(r.unit_mask[:u]), unit_rows=list(r.unit_rows[:u]),
+                      join_rows=list(r.join_rows[:u]), prep_ms=r.prep_ms, enum_ms=r.enum_ms, join_ms=r.join_ms,
+                      work_bytes=r.work_bytes, memory_bytes=r.memory_bytes)
+
+
+def decompose(query: Graph, max_unit_vertices: int = 12) -> list:
+    """Vertex masks of the units psm_match_join uses (host only)."""
+    qb = _QueryBuf(query)
+    n = C.c_uint32()
+    masks = (C.c_uint32 * N.MAX_UNITS)()
+    N.check(N.lib().psm_query_decompose(C.byref(qb.desc), int(max_unit_vertices), C.byref(n), masks))
+    return list(masks[: n.value])
+
+
+def hash_join(engine: Engine, r_rows: np.ndarray, r_vertex, s_rows: np.ndarray, s_vertex, vertex_label=None,
+              count_only: bool = False):
+    """One device hash join of host relations (R builds, S probes). Returns
+    (rows, out_vertex) or, with count_only, the number of rows."""
+    R = np.ascontiguousarray(r_rows, np.uint32).reshape(len(r_rows), len(r_vertex))
+    S = np.ascontiguousarray(s_rows, np.uint32).reshape(len(s_rows), len(s_vertex))
+    rv = np.ascontiguousarray(r_vertex, np.uint32)
+    sv = np.ascontiguousarray(s_vertex, np.uint32)
+    lab = None if vertex_label is None else np.ascontiguousarray(vertex_label, np.uint32)
+    labp = _u32p(lab) if lab is not None else None
+    n = C.c_uint64()
+    L = N.lib()
+    N.check(L.psm_hash_join(engine._h, _u32p(R), R.shape[0], R.shape[1], _u32p(rv), _u32p(S), S.shape[0], S.shape[1],
+                            _u32p(sv), labp, None, 0, None, None, C.byref(n)))
+    if count_only:
+        return n.value
+    total = n.value
+    ov = np.zeros(32, np.uint32)
+    oc = C.c_uint32()
+    out = np.empty((max(total, 1), 32), np.uint32)
+    N.check(L.psm_hash_join(engine._h, _u32p(R), R.shape[0], R.shape[1], _u32p(rv), _u32p(S), S.shape[0], S.shape[1],
+                            _u32p(sv), labp, _u32p(out), total, _u32p(ov), C.byref(oc), C.byref(n)))
+    w = oc.value
+    rows = np.frombuffer(out.tobytes()[: total * w * 4], np.uint32).reshape(total, w) if total else \
+        np.empty((0, w), np.uint32)
+    return rows, list(ov[:w])
+
+
+# --------------------------------------------------------------- serving --
+
+@dataclass
+class RequestResult:
+    ticket: int
+    count: int
+    status: int
+    overtime: bool
+    submit_ns: int
+    start_ns: int
+    done_ns: int
+    batch_size: int
+    lane: int
+    prep_ms: float
+    enum_ms: float
+
+    @property
+    def latency_ms(self) -> float:
+        return (self.done_ns - self.submit_ns) / 1e6
+
+
+class Server:
+    """Request loop over a resident data graph with continuous batching:
+    `lanes` batches run side by side, each admitting the queued requests
+    that fit its device-memory budget when it frees up."""
+
+    def __init__(self, data: DataGraph, method: str = "CFL_CFL_EXPLORE", cap: int = 0, time_limit: float = 60.0,
+                 lanes: int = 2, max_batch: int = 256, lane_arena_bytes: int = 8 << 30, full_gpu_lanes: bool = False,
+                 device: int = 0):
+        self.data = data  # keeps the graph alive
+        opt = options(method, cap, time_limit)
+        cfg = N.ServerConfig(lanes, max_batch, lane_arena_bytes, 1 if full_gpu_lanes else 0, 0)
+        self._h = C.c_void_p()
+        N.check(N.lib().psm_server_create(device, data._h, C.byref(opt), C.byref(cfg), C.byref(self._h)))
+
+    @staticmethod
+    def clock_ns() -> int:
+        return N.lib().psm_server_clock_ns()
+
+    def submit(self, query: Graph) -> int:
+        qb = _QueryBuf(query)
+        t = C.c_uint64()
+        N.check(N.lib().psm_server_submit(self._h, C.byref(qb.desc), C.byref(t)))
+        return t.value
+
+    def estimate(self, query: Graph):
+        qb = _QueryBuf(query)
+        b, budget = C.c_uint64(), C.c_uint64()
+        N.check(N.lib().psm_server_estimate(self._h, C.byref(qb.desc), C.byref(b), C.byref(budget)))
+        return b.value, budget.value
+
+    def poll(self, max_results: int = 4096, wait_s: float = 0.0):
+        buf = (N.RequestResult * max_results)()
+        n = C.c_uint32()
+        N.check(N.lib().psm_server_poll(self._h, buf, max_results, C.byref(n), float(wait_s)))
+        return [RequestResult(ticket=r.ticket, count=r.count, status=r.status, overtime=bool(r.overtime),
+                              submit_ns=r.submit_ns, start_ns=r.start_ns, done_ns=r.done_ns, batch_size=r.batch_size,
+                              lane=r.lane, prep_ms=r.prep_ms, enum_ms=r.enum_ms) for r in buf[: n.value]]
+
+    def pending(self):
+        q, r = C.c_uint64(), C.c_uint64()
+        N.check(N.lib().psm_server_pending(self._h, C.byref(q), C.byref(r)))
+        return q.value, r.value
+
+    def drain(self, n_expected: int, timeout_s: float = 600.0):
+        """Polls until n_expected results have arrived (or the timeout)."""
+        out = []
+        t_end = Server.clock_ns() + int(timeout_s * 1e9)
+        while len(out) < n_expected and Server.clock_ns() < t_end:
+            out += self.poll(wait_s=0.05)
+        return out
+
+    def close(self):
+        if self._h:
+            N.lib().psm_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

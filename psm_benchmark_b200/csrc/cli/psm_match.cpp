@@ -6,7 +6,11 @@
 // "[Thread 1] " like utility/statistics/Logs.h:88-96. The C-mode driver loop
 // mirrors split_C_test (matching/StudyPerformance.cpp:1039-1781): for every
 // entry of -threadnums and every FILTER_ORDER_ENGINE triple of -BackMethods,
-// one query run and one log block.
+// one query run and one log block. Q mode (-QorCandi Q, split_Q_test,
+// StudyPerformance.cpp:100-1037) runs the decomposition + hash-join path
+// (psm_match_join): units of at most -max_unit vertices (default 12) replace
+// the reference's -Qpattern decompositions, whose name is recorded; the
+// count does not depend on the decomposition.
 //
 // Differences a caller can see:
 //  - every engine name is accepted and served by the set-intersection
@@ -50,7 +54,7 @@ Flags parse_flags(int argc, char** argv) {
     static const char* keys[] = {"-a", "-i", "-q", "-d", "-d0", "-w0", "-filter", "-order", "-engine", "-num",
                                  "-time_limit", "-order_num", "-dis_file", "-csr", "-OutputFile", "-threadnums",
                                  "-split", "-schedule", "-QorCandi", "-Qpattern", "-JoinMethod", "-BackMethods",
-                                 "-device", "-arena_gb"};
+                                 "-device", "-arena_gb", "-max_unit"};
     Flags f;
     for (int i = 1; i + 1 < argc; ++i)
         for (const char* k : keys)
@@ -161,13 +165,14 @@ int main(int argc, char** argv) {
         os = &file;
     }
     Log log{os};
-    if (mode != "C") {
+    if (mode != "C" && mode != "Q") {
         log << "Error: The split mode is not defined.";
         log.end();
         return 1;
     }
     if (qpath.empty() || dpath.empty()) {
-        std::cerr << "usage: psm_match -d <data graph> -q <query graph> -QorCandi C|Q [reference flags]\n";
+        std::cerr << "usage: psm_match -d <data graph> -q <query graph> -QorCandi C|Q [reference flags] "
+                     "[-device i] [-arena_gb g] [-max_unit k]\n";
         return 2;
     }
     const std::string num = f.get("-num", "MAX"), tl = f.get("-time_limit", "60");
@@ -176,6 +181,7 @@ int main(int argc, char** argv) {
     const std::vector<std::string> methods = split(f.get("-BackMethods", "DPiso"), ',');
     const int device = std::atoi(f.get("-device", "0").c_str());
     const double arena_gb = std::atof(f.get("-arena_gb", "16").c_str());
+    const uint32_t max_unit = (uint32_t)std::atoi(f.get("-max_unit", "12").c_str());
 
     auto t0 = std::chrono::steady_clock::now();
     psm_graph* g = nullptr;
@@ -215,8 +221,13 @@ int main(int argc, char** argv) {
             log << "Maximum Embedding Number: " << num; log.end();
             log << "Time Limit: " << tl; log.end();
             log << "Num Threads: " << nt; log.end();
-            log << "Split Type: " << split_type; log.end();
-            log << "Schedule Type: " << schedule; log.end();
+            if (mode == "C") {
+                log << "Split Type: " << split_type; log.end();
+                log << "Schedule Type: " << schedule; log.end();
+            } else {
+                log << "QuerySplit Pattern: " << f.get("-Qpattern", "STAR"); log.end();
+                log << "Join Paradigm: " << f.get("-JoinMethod", "LEFTDEEP"); log.end();
+            }
             log << "Filter Type: " << ft; log.end();
             log << "Order Type: " << ot; log.end();
             log << "Engine Type: " << et; log.end();
@@ -245,16 +256,32 @@ int main(int argc, char** argv) {
             log << "-----"; log.end();
             log << "Generate a matching order..."; log.end();
             psm_result r{};
+            psm_join_result jr{};
             auto w0 = std::chrono::steady_clock::now();
-            int rc = psm_match(ctx, g, &q, &opt, &r);
+            int rc = mode == "C" ? psm_match(ctx, g, &q, &opt, &r) : psm_match_join(ctx, g, &q, &opt, max_unit, &jr);
             auto w1 = std::chrono::steady_clock::now();
             if (rc != PSM_OK && rc != PSM_ERR_TIMEOUT) {
                 std::cerr << "psm_match: " << psm_status_string(rc) << ": " << psm_last_error() << "\n";
                 exit_code = 1;
                 continue;
             }
-            log << "subgraph count == 1"; log.end();
-            log << "subgraph 0 vertices count == " << q.num_vertices; log.end();
+            double join_s = 0;
+            if (mode == "Q") {
+                // the join path's figures in the plain path's fields
+                r.count = jr.count;
+                r.prep_ms = jr.prep_ms;
+                r.enum_ms = jr.enum_ms;
+                r.memory_bytes = jr.memory_bytes;
+                r.overtime = rc == PSM_ERR_TIMEOUT;
+                join_s = jr.join_ms / 1e3;
+                log << "subgraph count == " << jr.units; log.end();
+                for (uint32_t k = 0; k < jr.units; ++k) {
+                    log << "subgraph " << k << " vertices count == " << __builtin_popcount(jr.unit_mask[k]); log.end();
+                }
+            } else {
+                log << "subgraph count == 1"; log.end();
+                log << "subgraph 0 vertices count == " << q.num_vertices; log.end();
+            }
             log << "-----"; log.end();
             log << "Enumerate..."; log.end();
             log << "schedule_type == " << schedule; log.end();
@@ -269,8 +296,8 @@ int main(int argc, char** argv) {
             log << "Generate query plan time (seconds): " << 0; log.end();
             log << "Enumerate time (seconds): " << enum_s; log.end();
             log << "Preprocessing time (seconds): " << prep_s; log.end();
-            log << "Join time (seconds): " << 0; log.end();
-            log << "Total time (seconds): " << prep_s + enum_s; log.end();
+            log << "Join time (seconds): " << join_s; log.end();
+            log << "Total time (seconds): " << prep_s + enum_s + join_s; log.end();
             log << "Memory cost (MB): " << r.memory_bytes / (double)(1024 * 1024); log.end();
             log << "#Embeddings: " << r.count; log.end();
             log << "Call Count: " << r.calls; log.end();

@@ -12,6 +12,9 @@
 #include <vector>
 
 #include "host.h"
+// after host.h (psm_b200.h first)
+#include "decompose.h"
+#include "join.h"
 
 int psm_graph_build(const uint32_t* off, const uint32_t* nbr, const uint32_t* labels, uint32_t V, psm_graph** out,
                     std::string* err);
@@ -85,9 +88,18 @@ struct psm_run {
     QState hq{};
     QDesc* hdesc = nullptr;  // host copy (order / labels)
     u32 n = 0;
+    size_t arena_free = 0;   // first arena byte not used by the run
 };
 
 int psm_fail(int code, const std::string& msg) { return fail(code, msg); }
+
+void psm_context_share_gpu(psm_context* ctx, u32 parts) {
+    if (!ctx || parts < 2) return;
+    ctx->enum_blocks = std::max(1, ctx->enum_blocks / (int)parts);
+    ctx->prep_block_blocks = std::max(1, ctx->prep_block_blocks / (int)parts);
+}
+
+u64 psm_context_free_bytes(const psm_context* ctx) { return ctx->arena_bytes - ctx->fixed_bytes; }
 
 int psm_run_internals(psm_run* r, RunInternals* out) {
     if (!r || !r->ctx || !r->d_q) return fail(PSM_ERR_ARG, "run is not alive");
@@ -184,7 +196,7 @@ void fill_result(const DevResult& r, float prep_ms, float enum_ms, u64 donations
 // Runs nq queries. grid_team: prepare the (single) query with the whole grid
 // (plain path); otherwise one block per query (batched path).
 int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, u32 nq, const psm_options& opt,
-                bool grid_team, psm_result* results, psm_run* keep) {
+                bool grid_team, psm_result* results, psm_run* keep, bool prep_only = false) {
     if (!ctx || !g || !qs || nq == 0) return fail(PSM_ERR_ARG, "null argument");
     if (ctx->run_live) return fail(PSM_ERR_ARG, "a psm_run is still alive on this context");
     CK(cudaSetDevice(ctx->device));
@@ -236,14 +248,18 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
                                  ctx->st));
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_enum_q, budget, opt.emit ? 1 : 0,
-                       ctx->enum_blocks, ctx->d_enum_cache, ctx->st));
+    if (!prep_only)
+        CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_enum_q, budget, opt.emit ? 1 : 0,
+                           ctx->enum_blocks, ctx->d_enum_cache, ctx->st));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     CK(psm_launch_gather(lay.d_q, nq, lay.d_res, ctx->st));
     std::vector<DevResult> res(nq);
     CK(cudaMemcpyAsync(res.data(), lay.d_res, sizeof(DevResult) * nq, cudaMemcpyDeviceToHost, ctx->st));
     EnumStats es{};
-    CK(psm_enum_read_ctl(ctx->d_enum_scratch, &es, ctx->st));
+    if (prep_only)
+        CK(cudaStreamSynchronize(ctx->st));
+    else
+        CK(psm_enum_read_ctl(ctx->d_enum_scratch, &es, ctx->st));
     const u32 enum_err = es.error;
     float prep_ms = 0, enum_ms = 0;
     CK(cudaEventElapsedTime(&prep_ms, ctx->ev[0], ctx->ev[1]));
@@ -302,6 +318,9 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
         keep->hdesc = new QDesc;
         memcpy(keep->hdesc, &descs[0], sizeof(QDesc));
         keep->n = descs[0].n;
+        DevArena top{};
+        CK(cudaMemcpy(&top, ctx->d_devarena, sizeof(top), cudaMemcpyDeviceToHost));
+        keep->arena_free = align_up(start + (size_t)std::min<u64>(top.top, top.cap) * sizeof(u32));
         ctx->run_live = true;
     }
     if (worst == PSM_ERR_INTERNAL) return fail(worst, enum_err ? "enumeration wait gave up" : "device error");
@@ -511,6 +530,350 @@ void psm_run_free(psm_run* r) {
     if (r->ctx) r->ctx->run_live = false;
     delete r->hdesc;
     delete r;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ join path --
+
+namespace {
+
+// Two-ended allocator over the free part of the arena: relations grow from
+// the bottom, per-join temporaries from the top (released after each join).
+struct Arena2 {
+    char* base;
+    size_t lo, hi;  // [lo, hi) is free
+    template <class T>
+    T* low(size_t count) {
+        size_t bytes = align_up(std::max<size_t>(count, 1) * sizeof(T));
+        if (lo + bytes > hi) return nullptr;
+        T* p = (T*)(base + lo);
+        lo += bytes;
+        return p;
+    }
+    template <class T>
+    T* high(size_t count) {
+        size_t bytes = align_up(std::max<size_t>(count, 1) * sizeof(T));
+        if (hi < lo + bytes) return nullptr;
+        hi -= bytes;
+        return (T*)(base + hi);
+    }
+};
+
+// A relation of partial embeddings in device memory: n rows of ncols data
+// vertex ids; column c holds query vertex vert[c].
+struct Rel {
+    u32* rows = nullptr;
+    u64 n = 0;
+    u32 ncols = 0;
+    u32 vert[PSM_MAXQ]{};
+};
+
+// Joins build side B and probe side P (keys: the query vertices in both).
+// count_only: *total receives the number of output rows; otherwise *out
+// holds them (probe columns, then B's non-key columns).
+int join_rels(psm_context* ctx, Arena2& ar, const u32* label, const Rel& B, const Rel& P, bool count_only, Rel* out,
+              u64* total, u64* peak_bytes) {
+    JoinSpec sp{};
+    sp.bcols = B.ncols;
+    sp.pcols = P.ncols;
+    for (u32 i = 0; i < B.ncols; ++i) {
+        int in_p = -1;
+        for (u32 j = 0; j < P.ncols; ++j)
+            if (P.vert[j] == B.vert[i]) in_p = (int)j;
+        if (in_p >= 0) {
+            if (sp.nk >= PSM_JOIN_MAX_KEYS) return fail(PSM_ERR_ARG, "too many join keys");
+            sp.bkey[sp.nk] = i;
+            sp.pkey[sp.nk] = (u32)in_p;
+            ++sp.nk;
+        } else {
+            u32 same = 0;
+            for (u32 j = 0; j < P.ncols; ++j)
+                if (!label || label[P.vert[j]] == label[B.vert[i]]) same |= 1u << j;
+            sp.bx[sp.nbx] = i;
+            sp.bx_same[sp.nbx] = same;
+            ++sp.nbx;
+        }
+    }
+    if (P.ncols + sp.nbx > PSM_MAXQ) return fail(PSM_ERR_ARG, "joined rows wider than 32 columns");
+    if (B.n >= 0x7FFFFFFFull) return fail(PSM_ERR_OOM, "join build side above 2^31 rows");
+    const size_t hi0 = ar.hi;
+    u64 cap = 64;
+    while (cap < 2 * B.n) cap <<= 1;
+    JoinTable t{};
+    t.mask = (u32)(cap - 1);
+    t.slots = ar.high<u32>(cap);
+    t.gcount = ar.high<u32>(cap);
+    t.gfill = ar.high<u32>(cap);
+    t.goff = ar.high<u64>(cap);
+    t.grp = ar.high<u32>(B.n);
+    t.members = ar.high<u32>(B.n);
+    t.scan_tmp = ar.high<u64>(psm_scan_tmp_bytes(cap) / sizeof(u64) + 1);
+    t.error = ar.high<u32>(1);
+    u64* d_total = ar.high<u64>(1);
+    if (!t.slots || !t.gcount || !t.gfill || !t.goff || !t.grp || !t.members || !t.scan_tmp || !t.error || !d_total)
+        return fail(PSM_ERR_OOM, "device arena exhausted (join table)");
+    CK(psm_join_build(B.rows, B.n, sp, t, ctx->st));
+    CK(cudaMemsetAsync(d_total, 0, sizeof(u64), ctx->st));
+    u64 n_out = 0;
+    if (count_only) {
+        CK(psm_join_probe(P.rows, P.n, B.rows, sp, t, nullptr, nullptr, nullptr, (unsigned long long*)d_total,
+                          ctx->st));
+        CK(cudaMemcpyAsync(&n_out, d_total, sizeof(u64), cudaMemcpyDeviceToHost, ctx->st));
+    } else {
+        u32* cnt = ar.high<u32>(P.n);
+        u64* off = ar.high<u64>(P.n);
+        u64* stmp = ar.high<u64>(psm_scan_tmp_bytes(P.n) / sizeof(u64) + 1);
+        if (!cnt || !off || !stmp) return fail(PSM_ERR_OOM, "device arena exhausted (join counts)");
+        CK(psm_join_probe(P.rows, P.n, B.rows, sp, t, cnt, nullptr, nullptr, nullptr, ctx->st));
+        CK(psm_excl_scan(cnt, P.n, off, stmp, d_total, ctx->st));
+        CK(cudaMemcpyAsync(&n_out, d_total, sizeof(u64), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        out->ncols = P.ncols + sp.nbx;
+        for (u32 j = 0; j < P.ncols; ++j) out->vert[j] = P.vert[j];
+        for (u32 x = 0; x < sp.nbx; ++x) out->vert[P.ncols + x] = B.vert[sp.bx[x]];
+        out->n = n_out;
+        out->rows = ar.low<u32>(n_out * out->ncols);
+        if (!out->rows) return fail(PSM_ERR_OOM, "device arena exhausted (joined rows)");
+        CK(psm_join_probe(P.rows, P.n, B.rows, sp, t, nullptr, out->rows, off, nullptr, ctx->st));
+    }
+    u32 err = 0;
+    CK(cudaMemcpyAsync(&err, t.error, sizeof(u32), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (err) return fail(PSM_ERR_INTERNAL, "join table overflow");
+    *total = n_out;
+    *peak_bytes = std::max<u64>(*peak_bytes, ar.lo + (hi0 - ar.hi));
+    ar.hi = hi0;
+    return PSM_OK;
+}
+
+// Adjacency masks of a query description (validated like the matching path:
+// simple, loop-free edges inside the vertex range).
+int query_adjacency(const psm_query_desc& q, u32* adj) {
+    if (q.num_vertices == 0 || q.num_vertices > PSM_MAXQ) return fail(PSM_ERR_ARG, "query size out of range");
+    for (u32 u = 0; u < q.num_vertices; ++u) adj[u] = 0;
+    for (u32 e = 0; e < q.num_edges; ++e) {
+        const u32 a = q.edges[2 * e], b = q.edges[2 * e + 1];
+        if (a >= q.num_vertices || b >= q.num_vertices || a == b) return fail(PSM_ERR_ARG, "bad query edge");
+        adj[a] |= 1u << b;
+        adj[b] |= 1u << a;
+    }
+    return PSM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int psm_query_decompose(const psm_query_desc* q, uint32_t max_unit_vertices, uint32_t* num_units,
+                        uint32_t* unit_masks) {
+    if (!q || !num_units || !unit_masks) return fail(PSM_ERR_ARG, "null argument");
+    u32 adj[PSM_MAXQ], cnt[PSM_MAXQ] = {};
+    int rc = query_adjacency(*q, adj);
+    if (rc) return rc;
+    Decomposition dec;
+    std::string err;
+    if (psm_decompose(q->num_vertices, adj, cnt, max_unit_vertices, &dec, &err)) return fail(PSM_ERR_ARG, err);
+    *num_units = dec.nunits;
+    for (u32 k = 0; k < dec.nunits; ++k) unit_masks[k] = dec.units[k].mask;
+    return PSM_OK;
+}
+
+int psm_match_join(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
+                   uint32_t max_unit_vertices, psm_join_result* res) {
+    if (!ctx || !g || !q || !opt || !res) return fail(PSM_ERR_ARG, "null argument");
+    memset(res, 0, sizeof(*res));
+    if (opt->emit) return fail(PSM_ERR_ARG, "the join path counts; emit is not supported");
+    u32 adj[PSM_MAXQ];
+    int rc = query_adjacency(*q, adj);
+    if (rc) return rc;
+    // 1. the whole query: filter, tables, order (no enumeration)
+    psm_run run;
+    psm_result pr{};
+    psm_options po = *opt;
+    po.cap = 0;
+    rc = run_queries(ctx, g, q, 1, po, true, &pr, &run, /*prep_only=*/true);
+    struct Release {
+        psm_run& r;
+        ~Release() {
+            if (r.ctx) r.ctx->run_live = false;
+            delete r.hdesc;
+        }
+    } release{run};
+    if (rc) return rc;
+    res->prep_ms = pr.prep_ms;
+    res->memory_bytes = pr.memory_bytes;
+    const QState& hq = run.hq;
+    // 2. units
+    Decomposition dec;
+    std::string err;
+    if (psm_decompose(q->num_vertices, adj, hq.cnt, max_unit_vertices, &dec, &err)) return fail(PSM_ERR_ARG, err);
+    const u32 U = dec.nunits;
+    res->units = U;
+    for (u32 k = 0; k < U; ++k) res->unit_mask[k] = dec.units[k].mask;
+    if (hq.empty) {
+        res->status = PSM_OK;
+        return PSM_OK;  // some candidate set is empty: no embedding
+    }
+    Arena2 ar{ctx->arena, run.arena_free, ctx->arena_bytes};
+    std::vector<QState> uq(U, hq);
+    for (u32 k = 0; k < U; ++k) {
+        QState& s = uq[k];
+        const UnitPlan& up = dec.units[k];
+        for (u32 i = 0; i < PSM_MAXQ; ++i) s.order[i] = i < up.n ? up.order[i] : 0u;
+        s.n_enum = up.n;
+        s.emit_by_depth = 1;
+        s.emit_buf = nullptr;
+        s.emit_cap_rows = 0;
+        s.emit_rows = 0;
+        s.count = s.calls = s.alg_bytes = 0;
+        s.cap = 0;
+        s.stop = s.overtime = 0;
+        s.done_ns = 0;
+        s.trace = nullptr;
+    }
+    QState* d_uq = ar.low<QState>(U);
+    char* d_enum_q = ar.low<char>(psm_enum_query_bytes(U));
+    DevResult* d_res = ar.low<DevResult>(U);
+    u32** d_bufs = ar.low<u32*>(U);
+    u64* d_caps = ar.low<u64>(U);
+    if (!d_uq || !d_enum_q || !d_res || !d_bufs || !d_caps) return fail(PSM_ERR_OOM, "device arena exhausted (units)");
+    const u64 budget = budget_ns(*opt);
+    CK(cudaMemcpyAsync(d_uq, uq.data(), sizeof(QState) * U, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    CK(psm_launch_unit_plan(g->dev, d_uq, U, ctx->st));
+    // 3. count every unit, then emit every unit (one launch each)
+    std::vector<DevResult> dr(U);
+    auto run_units = [&](int emit) -> int {
+        CK(psm_launch_enum(g->dev, d_uq, U, ctx->d_enum_scratch, d_enum_q, budget, emit, ctx->enum_blocks,
+                           ctx->d_enum_cache, ctx->st));
+        CK(psm_launch_gather(d_uq, U, d_res, ctx->st));
+        CK(cudaMemcpyAsync(dr.data(), d_res, sizeof(DevResult) * U, cudaMemcpyDeviceToHost, ctx->st));
+        EnumStats es{};
+        CK(psm_enum_read_ctl(ctx->d_enum_scratch, &es, ctx->st));
+        if (es.error) return fail(PSM_ERR_INTERNAL, "enumeration wait gave up");
+        for (u32 k = 0; k < U; ++k) {
+            if (dr[k].overtime) return fail(PSM_ERR_TIMEOUT, "time limit reached (units)");
+            if (dr[k].status != PSM_DEV_OK) return fail(PSM_ERR_INTERNAL, "unit enumeration failed");
+        }
+        return PSM_OK;
+    };
+    rc = run_units(0);
+    if (rc) return rc;
+    u64 used = 0;
+    for (u32 k = 0; k < U; ++k) {
+        res->unit_rows[k] = dr[k].count;
+    }
+    if (U == 1) {
+        CK(cudaEventRecord(ctx->ev[1], ctx->st));
+        CK(cudaEventSynchronize(ctx->ev[1]));
+        float ms = 0;
+        CK(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+        res->enum_ms = ms;
+        res->join_rows[0] = dr[0].count;
+        res->count = opt->cap && dr[0].count > opt->cap ? opt->cap : dr[0].count;
+        res->status = PSM_OK;
+        return PSM_OK;
+    }
+    std::vector<u32*> bufs(U);
+    std::vector<u64> caps(U);
+    for (u32 k = 0; k < U; ++k) {
+        caps[k] = dr[k].count;
+        bufs[k] = ar.low<u32>(dr[k].count * dec.units[k].n);
+        if (!bufs[k]) return fail(PSM_ERR_OOM, "device arena exhausted (unit embeddings)");
+    }
+    CK(cudaMemcpyAsync(d_bufs, bufs.data(), sizeof(u32*) * U, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(d_caps, caps.data(), sizeof(u64) * U, cudaMemcpyHostToDevice, ctx->st));
+    CK(psm_launch_unit_emit(d_uq, U, d_bufs, d_caps, ctx->st));
+    rc = run_units(1);
+    if (rc) return rc;
+    for (u32 k = 0; k < U; ++k)
+        if (dr[k].emit_rows != caps[k]) return fail(PSM_ERR_INTERNAL, "unit emission differs from its count");
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    // 4. left-deep joins in unit order; the last one is counted
+    const u32* label = run.hdesc->label;
+    Rel acc;
+    acc.rows = bufs[0];
+    acc.n = caps[0];
+    acc.ncols = dec.units[0].n;
+    for (u32 i = 0; i < acc.ncols; ++i) acc.vert[i] = dec.units[0].order[i];
+    res->join_rows[0] = acc.n;
+    u64 total = acc.n;
+    for (u32 k = 1; k < U; ++k) {
+        Rel unit;
+        unit.rows = bufs[k];
+        unit.n = caps[k];
+        unit.ncols = dec.units[k].n;
+        for (u32 i = 0; i < unit.ncols; ++i) unit.vert[i] = dec.units[k].order[i];
+        const bool last = k + 1 == U;
+        // build on the smaller side
+        const bool build_acc = acc.n <= unit.n;
+        Rel next;
+        rc = join_rels(ctx, ar, label, build_acc ? acc : unit, build_acc ? unit : acc, last, &next, &total, &used);
+        if (rc) return rc;
+        res->join_rows[k] = total;
+        if (!last) acc = next;
+        if (total == 0) {
+            for (u32 j = k + 1; j < U; ++j) res->join_rows[j] = 0;
+            break;
+        }
+    }
+    CK(cudaEventRecord(ctx->ev[2], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[2]));
+    float e_ms = 0, j_ms = 0;
+    CK(cudaEventElapsedTime(&e_ms, ctx->ev[0], ctx->ev[1]));
+    CK(cudaEventElapsedTime(&j_ms, ctx->ev[1], ctx->ev[2]));
+    res->enum_ms = e_ms;
+    res->join_ms = j_ms;
+    res->work_bytes = std::max<u64>(used, ar.lo) - run.arena_free;
+    res->count = opt->cap && total > opt->cap ? opt->cap : total;
+    res->status = PSM_OK;
+    return PSM_OK;
+}
+
+int psm_hash_join(psm_context* ctx, const uint32_t* r_rows, uint64_t r_n, uint32_t r_cols, const uint32_t* r_vertex,
+                  const uint32_t* s_rows, uint64_t s_n, uint32_t s_cols, const uint32_t* s_vertex,
+                  const uint32_t* vertex_label, uint32_t* out_rows, uint64_t out_capacity, uint32_t* out_vertex,
+                  uint32_t* out_cols, uint64_t* out_n) {
+    if (!ctx || !r_vertex || !s_vertex || !out_n || (r_n && !r_rows) || (s_n && !s_rows))
+        return fail(PSM_ERR_ARG, "null argument");
+    if (r_cols == 0 || s_cols == 0 || r_cols > PSM_MAXQ || s_cols > PSM_MAXQ) return fail(PSM_ERR_ARG, "bad widths");
+    for (u32 i = 0; i < r_cols; ++i)
+        if (r_vertex[i] >= PSM_MAXQ) return fail(PSM_ERR_ARG, "query vertex id out of range");
+    for (u32 i = 0; i < s_cols; ++i)
+        if (s_vertex[i] >= PSM_MAXQ) return fail(PSM_ERR_ARG, "query vertex id out of range");
+    if (ctx->run_live) return fail(PSM_ERR_ARG, "a psm_run is still alive on this context");
+    CK(cudaSetDevice(ctx->device));
+    Arena2 ar{ctx->arena, ctx->fixed_bytes, ctx->arena_bytes};
+    Rel R, S;
+    R.n = r_n;
+    R.ncols = r_cols;
+    S.n = s_n;
+    S.ncols = s_cols;
+    for (u32 i = 0; i < r_cols; ++i) R.vert[i] = r_vertex[i];
+    for (u32 i = 0; i < s_cols; ++i) S.vert[i] = s_vertex[i];
+    R.rows = ar.low<u32>(r_n * r_cols);
+    S.rows = ar.low<u32>(s_n * s_cols);
+    if (!R.rows || !S.rows) return fail(PSM_ERR_OOM, "device arena exhausted (relations)");
+    if (r_n) CK(cudaMemcpyAsync(R.rows, r_rows, r_n * r_cols * sizeof(u32), cudaMemcpyHostToDevice, ctx->st));
+    if (s_n) CK(cudaMemcpyAsync(S.rows, s_rows, s_n * s_cols * sizeof(u32), cudaMemcpyHostToDevice, ctx->st));
+    u32 lab[PSM_MAXQ] = {};
+    if (vertex_label)
+        for (u32 i = 0; i < r_cols; ++i) lab[r_vertex[i]] = vertex_label[r_vertex[i]];
+    if (vertex_label)
+        for (u32 i = 0; i < s_cols; ++i) lab[s_vertex[i]] = vertex_label[s_vertex[i]];
+    Rel out;
+    u64 total = 0, used = 0;
+    int rc = join_rels(ctx, ar, vertex_label ? lab : nullptr, R, S, out_rows == nullptr, &out, &total, &used);
+    if (rc) return rc;
+    *out_n = total;
+    if (!out_rows) return PSM_OK;
+    if (out_cols) *out_cols = out.ncols;
+    if (out_vertex)
+        for (u32 i = 0; i < out.ncols; ++i) out_vertex[i] = out.vert[i];
+    if (out_capacity < total) return fail(PSM_ERR_ARG, "output buffer too small");
+    if (total) CK(cudaMemcpy(out_rows, out.rows, total * out.ncols * sizeof(u32), cudaMemcpyDeviceToHost));
+    return PSM_OK;
 }
 
 }  // extern "C"

@@ -458,8 +458,13 @@ __device__ u64 emit_last(QState& q, const DevGraph& g, u32 d, WarpStack* ws, u64
             u64 row = base + __popc(bal & ((1u << lane) - 1u));
             if (row < q.emit_cap_rows) {
                 u32* out = q.emit_buf + row * n;
-                for (u32 i = 0; i < d; ++i) out[q.order[i]] = g.orig[ws->vid[i]];
-                out[u] = g.orig[list_d[p]];
+                if (q.emit_by_depth) {
+                    for (u32 i = 0; i < d; ++i) out[i] = ws->vid[i];
+                    out[d] = list_d[p];
+                } else {
+                    for (u32 i = 0; i < d; ++i) out[q.order[i]] = g.orig[ws->vid[i]];
+                    out[u] = g.orig[list_d[p]];
+                }
             }
         }
         c += k;
@@ -850,7 +855,7 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
 __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws, EnumCtl* ctl, Slot* slots, bool emit,
                     u64& count, u64& bytes, u64& calls, u32& iter) {
     const u32 lane = lane_id();
-    const u32 n = q.desc->n;
+    const u32 n = q.n_enum;
     u32 d = d0;
     u64 bytes_l = 0, calls_l = 0;  // per-lane parts, summed at the end
     bool go = true;
@@ -958,7 +963,7 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
                          bool emit) {
     const u32 lane = lane_id();
     QState& q = qs[t.qi];
-    const u32 n = q.desc->n;
+    const u32 n = q.n_enum;
     if (warp_ld_volatile_u32(&q.stop)) return;
     u64 count = 0, bytes = 0, calls = 0;
     u32 iter = 0;
@@ -969,7 +974,8 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
         if (emit) {
             for (u32 i = t.b + lane; i < t.e; i += 32) {
                 unsigned long long r = atomicAdd((unsigned long long*)&q.emit_rows, 1ull);
-                if (r < q.emit_cap_rows) q.emit_buf[r] = g.orig[q.list[q.order[0]][i]];
+                const u32 v = q.list[q.order[0]][i];
+                if (r < q.emit_cap_rows) q.emit_buf[r] = q.emit_by_depth ? v : g.orig[v];
             }
         }
         publish(q, count, bytes, calls);
@@ -1193,7 +1199,7 @@ __global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, 
             const QState& q = qs[i];
             PoolInfo pi{KIND_RANGE, 0, 1, 0};
             if (q.status == PSM_DEV_OK && !q.stop && q.root_cnt > 0) {
-                const u32 n = q.desc->n;
+                const u32 n = q.n_enum;
                 if (n >= 4) {
                     const u32 tb = q.bn_tab[1][0];
                     pi.kind = KIND_EDGES;

@@ -107,6 +107,25 @@ int psm_graph_build(const uint32_t* off, const uint32_t* nbr, const uint32_t* la
         }
         std::sort(dst, dst + d);
     }
+    g->lab_deg.assign(L, 0);
+    if (L <= psm_graph::LAB_PAIR_MAX) g->lab_pair.assign((size_t)L * L, 0);
+    for (u32 i = 0; i < V; ++i) {
+        const u32 a = labels[orig[i]];
+        g->lab_deg[a] += ioff[i + 1] - ioff[i];
+        if (!g->lab_pair.empty()) {
+            u64* row = g->lab_pair.data() + (size_t)a * L;
+            // neighbours are sorted by internal id, i.e. grouped by label:
+            // one run per label present
+            const u32* r0 = inbr.data() + ioff[i];
+            const u32* r1 = inbr.data() + ioff[i + 1];
+            while (r0 < r1) {
+                const u32 b = (u32)(std::upper_bound(g->lab_off.begin(), g->lab_off.end(), *r0) - g->lab_off.begin()) - 1;
+                const u32* e = std::lower_bound(r0, r1, g->lab_off[b + 1]);
+                row[b] += (u64)(e - r0);
+                r0 = e;
+            }
+        }
+    }
     cudaGetDevice(&g->device);
     int rc;
     if ((rc = upload(&g->d_off, ioff.data(), ioff.size(), err)) || (rc = upload(&g->d_nbr, inbr.data(), nnz, err)) ||

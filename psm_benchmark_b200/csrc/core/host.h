@@ -21,7 +21,18 @@ struct psm_graph {
     u32* d_lab_off = nullptr;
     u32* d_orig = nullptr;
     DevGraph dev{};
+    // For memory estimates: sum of degrees per label, and (when L <=
+    // LAB_PAIR_MAX) the number of directed edges per label pair.
+    static constexpr u32 LAB_PAIR_MAX = 1024;
+    std::vector<u64> lab_deg;
+    std::vector<u64> lab_pair;  // [L * L]: edges from label a to label b at a * L + b
     u32 freq(u32 l) const { return l < L ? lab_off[l + 1] - lab_off[l] : 0u; }
+    // Upper bound on the entries of a candidate-edge table from label a to b.
+    u64 pair_edges(u32 a, u32 b) const {
+        if (a >= L || b >= L) return 0;
+        if (!lab_pair.empty()) return lab_pair[(u64)a * L + b];
+        return std::min(lab_deg[a], lab_deg[b]);
+    }
 };
 
 // Records msg as this thread's last error and returns code.
@@ -37,6 +48,12 @@ struct RunInternals {
     u32 emit;
 };
 int psm_run_internals(psm_run* run, RunInternals* out);
+
+// Sizes the context's persistent grids to 1/parts of the GPU (serving lanes
+// that run side by side).
+void psm_context_share_gpu(psm_context* ctx, u32 parts);
+// Arena bytes available to a batch (the arena minus its fixed region).
+u64 psm_context_free_bytes(const psm_context* ctx);
 
 // Builds the device query descriptor (validation, NLF lists, CFL plans).
 // Returns PSM_OK or PSM_ERR_ARG with *err set.
@@ -64,3 +81,5 @@ cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch
 cudaError_t psm_enum_max_blocks(int* blocks);
 cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st);
 cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st);
+cudaError_t psm_launch_unit_plan(const DevGraph& g, QState* qs, u32 nq, cudaStream_t st);
+cudaError_t psm_launch_unit_emit(QState* qs, u32 nq, u32* const* bufs, const u64* caps, cudaStream_t st);

@@ -865,12 +865,13 @@ __device__ void cfl_order_select(QState& q, const u32* pw) {
 // lane i handles depth i; all loops are warp-uniform.
 __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
     const QDesc* d = q.desc;
-    const u32 n = d->n;
+    const u32 nv = d->n;       // query vertices
+    const u32 n = q.n_enum;    // depths (n_enum < nv for a decomposition unit)
     const u32 lane = lane_id();
     const bool act = lane < n;
     const u32 u = act ? q.order[lane] : 0u;          // vertex at depth lane
     const u32 lab = act ? d->label[u] : 0xFFFFFFFFu;  // its label
-    u32 depth_of = 0;                                 // depth of vertex `lane`
+    u32 depth_of = 0;                                 // depth of vertex `lane` (if ordered)
     for (u32 j = 0; j < n; ++j)
         if (__shfl_sync(FULL_MASK, u, j) == lane) depth_of = j;
     u32 seen_incl = act ? (1u << u) : 0u;  // vertices at depths <= lane
@@ -881,13 +882,15 @@ __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
     const u32 seen = seen_incl & ~(act ? (1u << u) : 0u);
     const u32 m = act ? (d->adj[u] & seen) : 0u;
     u32 k = 0, same = 0;
-    for (u32 b = 0; b < n; ++b) {
+    for (u32 b = 0; b < nv; ++b) {  // b: query vertex
         const u32 db = __shfl_sync(FULL_MASK, depth_of, b);
         if ((m >> b) & 1u) {
             q.bn_depth[lane][k] = db;
             q.bn_tab[lane][k] = table_base(q, b, u);
             ++k;
         }
+    }
+    for (u32 b = 0; b < n; ++b) {  // b: depth
         const u32 lb = __shfl_sync(FULL_MASK, lab, b);
         if (b < lane && lb == lab) same |= 1u << b;
     }
@@ -913,18 +916,19 @@ __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
         const u32 bal = __ballot_sync(FULL_MASK, act && cm != 0 && cdep >= x);
         if (lane == x) inval = bal;
     }
+    if (lane < nv) q.cbase[lane] = bucket_base(g, d->label[lane]);  // by query vertex
     if (act) {
         q.nbn[lane] = k;
         q.same_mask[lane] = same;
-        q.cbase[lane] = bucket_base(g, d->label[lane]);
         q.cmask[lane] = cm;
         q.crow[lane] = crow;
         q.cinval[lane] = inval;
     }
     if (lane == 0) q.bm_depths = bm_depths;
     // memory cost: candidates of every vertex, both tables of every edge
+    // (the query's; a unit keeps the value it was given)
     u64 mem = 0;
-    if (act) {
+    if (lane < nv && n == nv) {
         const u32 a = lane;
         mem += (u64)q.cnt[a] * 4u;
         u32 mb = d->adj[a] & ~((2u << a) - 1u);  // neighbours b > a
@@ -938,7 +942,7 @@ __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
     }
     mem = warp_sum64(mem);
     if (lane == 0) {
-        q.memory_bytes = mem;
+        if (n == nv) q.memory_bytes = mem;
         q.root_cnt = q.empty ? 0u : q.cnt[q.order[0]];
     }
 }
@@ -993,6 +997,7 @@ __device__ bool run_step(Team& t, const DevGraph& g, QState& q, DevArena* arena,
             q.stop = 0;
             q.overtime = 0;
             q.emit_rows = 0;
+            q.n_enum = d->n;
             q.table_nnz = 0;
             q.memory_bytes = 0;
             q.root_cnt = 0;
@@ -1335,4 +1340,45 @@ cudaError_t psm_prep_grid_max_blocks(int threads, int* blocks) {
     if (e != cudaSuccess) return e;
     *blocks = sms * (per_sm < 1 ? 1 : per_sm);
     return cudaSuccess;
+}
+
+// ------------------------------------------------------ decomposition units --
+//
+// A decomposition unit is enumerated on a copy of its query's QState whose
+// order lists only the unit's vertices (n_enum of them); the unit reuses the
+// query's candidate sets and tables. These kernels recompute the enumeration
+// plan of such copies and arm their emission buffers.
+
+namespace {
+
+__global__ void unit_plan_kernel(DevGraph g, QState* qs, u32 nq) {
+    if (blockIdx.x < nq && threadIdx.x < 32) enum_plan_warp(g, qs[blockIdx.x]);
+}
+
+__global__ void unit_emit_kernel(QState* qs, u32 nq, u32* const* bufs, const u64* caps) {
+    for (u32 i = threadIdx.x; i < nq; i += blockDim.x) {
+        QState& q = qs[i];
+        q.emit_buf = bufs[i];
+        q.emit_cap_rows = caps[i];
+        q.emit_rows = 0;
+        q.emit_by_depth = 1;
+        q.count = 0;
+        q.calls = 0;
+        q.alg_bytes = 0;
+        q.stop = 0;
+        q.overtime = 0;
+        q.done_ns = 0;
+    }
+}
+
+}  // namespace
+
+cudaError_t psm_launch_unit_plan(const DevGraph& g, QState* qs, u32 nq, cudaStream_t st) {
+    unit_plan_kernel<<<nq, 32, 0, st>>>(g, qs, nq);
+    return cudaGetLastError();
+}
+
+cudaError_t psm_launch_unit_emit(QState* qs, u32 nq, u32* const* bufs, const u64* caps, cudaStream_t st) {
+    unit_emit_kernel<<<1, 256, 0, st>>>(qs, nq, bufs, caps);
+    return cudaGetLastError();
 }

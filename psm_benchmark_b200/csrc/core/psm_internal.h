@@ -163,7 +163,13 @@ struct QState {
     u32 stop;               // cap reached / error -> stop enumerating
     u32 overtime;
     u64 done_ns;            // %globaltimer when the cap was reached (0 if never)
-    // emit mode
+    // Depths the enumerator runs: the query's n, or the size of a
+    // decomposition unit whose order lists only the unit's vertices (the
+    // unit reuses the query's candidates and tables).
+    u32 n_enum;
+    // emit mode (rows of n_enum data ids: by query vertex in original ids,
+    // or, with emit_by_depth, by depth in internal ids)
+    u32 emit_by_depth;
     u32* emit_buf;
     u64 emit_cap_rows;
     u64 emit_rows;

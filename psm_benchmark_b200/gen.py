@@ -201,3 +201,34 @@ SERVE_WEIGHTS = np.array([0.3, 0.25, 0.2, 0.1, 0.1, 0.05])
 def serve_sizes(num_queries: int, seed: int):
     rng = np.random.Generator(np.random.PCG64(seed))
     return rng.choice(SERVE_SIZES, size=num_queries, p=SERVE_WEIGHTS)
+
+
+def join_sizes(num_queries: int, seed: int):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return rng.integers(24, 33, size=num_queries)
+
+
+def join(num_queries: int = 200, scale: int = 22, graph: Graph | None = None) -> Workload:
+    """Decomposition + hash join: R-MAT scale 22, edge factor 16, 64
+    Zipf(1.0) labels; 24..32-vertex queries, joined from units of <= 12
+    vertices."""
+    g = graph if graph is not None else make_graph("rmat", 4, scale=scale, edge_factor=16, num_labels=64,
+                                                   zipf_s=1.0)
+    w = Workload("join", 4, g, filter="CFL", order="CFL", engine="EXPLORE", cap=0)
+    w.queries = make_queries(g, join_sizes(num_queries, w.seed), w.seed)
+    return w
+
+
+def serve(num_queries: int = 50000, scale: int = 24, graph: Graph | None = None) -> Workload:
+    """Serving: R-MAT scale 24, edge factor 16, 128 uniform labels; query sizes
+    {4,8,12,16,24,32} weighted .3/.25/.2/.1/.1/.05; cap 1e9."""
+    g = graph if graph is not None else make_graph("rmat", 5, scale=scale, edge_factor=16, num_labels=128)
+    w = Workload("serve", 5, g, filter="CFL", order="CFL", engine="EXPLORE", cap=10**9)
+    w.queries = make_queries(g, serve_sizes(num_queries, w.seed), w.seed)
+    return w
+
+
+def poisson_arrivals(num: int, rate_per_s: float, seed: int) -> np.ndarray:
+    """Arrival times (s) of a Poisson stream of `num` requests."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    return np.cumsum(rng.exponential(1.0 / rate_per_s, size=num))

@@ -23,7 +23,11 @@ EXPORTS = [
     "psm_context_create", "psm_context_free",
     "psm_match", "psm_run_create", "psm_run_candidates", "psm_run_table", "psm_run_order",
     "psm_run_embeddings", "psm_run_free", "psm_match_batch", "psm_run_recount_noalloc",
+    "psm_match_join", "psm_query_decompose", "psm_hash_join",
+    "psm_server_create", "psm_server_submit", "psm_server_poll", "psm_server_pending", "psm_server_estimate",
+    "psm_server_clock_ns", "psm_server_destroy",
 ]
+MAX_UNITS = 32
 
 
 class PsmError(RuntimeError):
@@ -54,6 +58,24 @@ class Result(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("lanes", C.c_uint32), ("max_batch", C.c_uint32), ("lane_arena_bytes", C.c_uint64),
+                ("full_gpu_lanes", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("count", C.c_uint64), ("status", C.c_uint32), ("overtime", C.c_uint32),
+                ("submit_ns", C.c_uint64), ("start_ns", C.c_uint64), ("done_ns", C.c_uint64),
+                ("batch_size", C.c_uint32), ("lane", C.c_uint32), ("prep_ms", C.c_double), ("enum_ms", C.c_double)]
+
+
+class JoinResult(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("units", C.c_uint32), ("status", C.c_uint32),
+                ("unit_mask", C.c_uint32 * MAX_UNITS), ("unit_rows", C.c_uint64 * MAX_UNITS),
+                ("join_rows", C.c_uint64 * MAX_UNITS), ("prep_ms", C.c_double), ("enum_ms", C.c_double),
+                ("join_ms", C.c_double), ("work_bytes", C.c_uint64), ("memory_bytes", C.c_uint64)]
+
+
 @lru_cache(maxsize=1)
 def lib():
     if not LIB_PATH.exists():
@@ -82,6 +104,18 @@ def lib():
         "psm_match_batch": ([vp, vp, C.POINTER(QueryDesc), C.c_uint32, C.POINTER(Options), C.POINTER(Result)],
                             C.c_int),
         "psm_run_recount_noalloc": ([vp, C.c_uint64, C.c_double, C.POINTER(C.c_uint64), u32p], C.c_int),
+        "psm_match_join": ([vp, vp, C.POINTER(QueryDesc), C.POINTER(Options), C.c_uint32, C.POINTER(JoinResult)],
+                           C.c_int),
+        "psm_query_decompose": ([C.POINTER(QueryDesc), C.c_uint32, u32p, u32p], C.c_int),
+        "psm_server_create": ([C.c_int, vp, C.POINTER(Options), C.POINTER(ServerConfig), C.POINTER(vp)], C.c_int),
+        "psm_server_submit": ([vp, C.POINTER(QueryDesc), C.POINTER(C.c_uint64)], C.c_int),
+        "psm_server_poll": ([vp, C.POINTER(RequestResult), C.c_uint32, u32p, C.c_double], C.c_int),
+        "psm_server_pending": ([vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
+        "psm_server_estimate": ([vp, C.POINTER(QueryDesc), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
+        "psm_server_clock_ns": ([], C.c_uint64),
+        "psm_server_destroy": ([vp], None),
+        "psm_hash_join": ([vp, u32p, C.c_uint64, C.c_uint32, u32p, u32p, C.c_uint64, C.c_uint32, u32p, u32p, u32p,
+                           C.c_uint64, u32p, u32p, C.POINTER(C.c_uint64)], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

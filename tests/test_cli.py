@@ -95,3 +95,24 @@ def test_unsupported_filter_is_reported(cli, tmp_path):
     assert "The specified filter type 'DPiso' is not supported." in text
     blocks = parse_blocks(text)
     assert len(blocks) == 1 and int(blocks[0]["#Embeddings"]) == counts[0]
+
+
+@pytest.mark.gpu
+def test_hprd_counts_through_cli_q_mode(cli, tmp_path):
+    """-QorCandi Q (decomposition + join) gives the same #Embeddings."""
+    g, qs, counts = hprd()
+    data = tmp_path / "d.txt"
+    g.write_text(data)
+    for i in (0, 3, 6):
+        qf = tmp_path / f"q{i}.txt"
+        qs[i].write_text(qf)
+        log = tmp_path / f"q{i}.log"
+        p = run(cli, ["-d", str(data), "-q", str(qf), "-QorCandi", "Q", "-Qpattern", "STAR", "-JoinMethod", "LEFTDEEP",
+                      "-threadnums", "1", "-OutputFile", str(log), "-BackMethods", "CFL_CFL_EXPLORE", "-max_unit", "4"])
+        assert p.returncode == 0, p.stderr
+        text = log.read_text()
+        blocks = parse_blocks(text)
+        assert len(blocks) == 1
+        assert int(blocks[0]["#Embeddings"]) == counts[i]
+        assert blocks[0]["QuerySplit Pattern"] == "STAR"
+        assert int(re.search(r"subgraph count == (\d+)", text).group(1)) >= 2
