@@ -290,10 +290,8 @@ def ours_arm(args, world, rank, local):
     barrier()
     wall = time.perf_counter() - t0
     clk = clocks.stop()
-    if dist is not None:
-        t = torch.tensor([dev_ms, wall], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms, wall = float(t[0]), float(t[1])
+    from psm_benchmark_b200.replicas import max_over_ranks
+    dev_ms, wall = max_over_ranks([dev_ms, wall], dist, device=f"cuda:{local}")
     nq = len(w.queries)
     value = world * nq * args.steps / (dev_ms / 1e3)
     e2e = world * nq * args.steps / wall
@@ -351,6 +349,211 @@ def ours_arm(args, world, rank, local):
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------ other workloads --
+#
+# `--workload batched|join|serve` measure the other rows of the path, each
+# with its own JSON line: the batched path on 2,000 mixed queries, the
+# decomposition + join path against the reference's own join path, and the
+# serving loop at offered loads of 50 / 80 / 95 % of its saturation rate.
+
+def _torch_setup(local):
+    import torch
+    torch.cuda.set_device(local)
+    return torch
+
+
+def batched_leg(args, local):
+    torch = _torch_setup(local)
+    from psm_benchmark_b200 import api, gen
+    w = gen.batched(num_queries=args.queries if args.queries != 200 else 2000, scale=args.scale)
+    # candidate buffers of 2,000 queries take about 40 GB
+    eng = api.Engine(device=local, arena_bytes=max(args.arena_gb, 64) << 30)
+    dg = api.DataGraph.from_graph(w.graph)
+    flush = torch.empty(256 << 20 >> 2, dtype=torch.float32, device=f"cuda:{local}")
+    nq = len(w.queries)
+
+    def batched():
+        flush_l2(flush)
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        res = api.match_batch(eng, dg, w.queries, w.method, cap=w.cap, time_limit=args.time_limit)
+        return res, time.perf_counter() - t
+
+    for _ in range(args.warmup):
+        batched()
+    clocks = ClockSampler(local).start()
+    dev, wall, res = 0.0, 0.0, None
+    for _ in range(args.steps):
+        res, t = batched()
+        dev += res[0].prep_ms + res[0].enum_ms
+        wall += t
+    clk = clocks.stop()
+    # the plain path on the same queries (one warm pass, one timed pass)
+    for q in w.queries[:50]:
+        api.match(eng, dg, q, w.method, cap=w.cap, time_limit=args.time_limit)
+    flush_l2(flush)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    plain = [api.match(eng, dg, q, w.method, cap=w.cap, time_limit=args.time_limit) for q in w.queries]
+    p_wall = time.perf_counter() - t
+    p_dev = sum(r.prep_ms + r.enum_ms for r in plain)
+    if [r.count for r in plain] != [r.count for r in res]:
+        raise SystemExit("batched counts differ from the plain path")
+    value = nq * args.steps / (dev / 1e3)
+    sizes = {}
+    for q, r in zip(w.queries, plain):
+        sizes.setdefault(q.num_vertices, []).append(r.prep_ms + r.enum_ms)
+    line = {"metric": "queries/sec (batched GPU path, mixed 4-32-vertex queries, CFL_CFL_EXPLORE, cap 1e9)",
+            "value": value, "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dev / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "batched_rmat_s20", "queries_per_step": nq,
+                       "query_sizes": "uniform over {4,6,8,12,16,24,32}", "method": w.method, "cap": w.cap,
+                       "l2": "flushed (256 MiB write) before every step"},
+            "embeddings_per_s": sum(r.count for r in res) * args.steps / (dev / 1e3),
+            "e2e": {"value": nq * args.steps / wall, "unit": "queries/s"},
+            "gpu_launches": 4 * args.steps,
+            "plain": {"value": nq / (p_dev / 1e3), "e2e": nq / p_wall, "unit": "queries/s",
+                      "latency_ms_by_size": {str(k): {"p50": float(np.percentile(v, 50)),
+                                                      "p99": float(np.percentile(v, 99))}
+                                             for k, v in sorted(sizes.items())}},
+            "speedup_vs_plain": value / (nq / (p_dev / 1e3)),
+            "e2e_speedup_vs_plain": (nq * args.steps / wall) / (nq / p_wall),
+            "counts_equal_plain": True, "clocks": clk}
+    print(json.dumps(line))
+
+
+def join_leg(args, local):
+    _torch_setup(local)
+    from psm_benchmark_b200 import api, gen
+    from psm_benchmark_b200.graphs import Graph
+    golden = ROOT / "tests" / "golden"
+    ref = json.loads((golden / "join_ref.json").read_text())
+    z = np.load(golden / "hprd15.npz")
+    hg = Graph(off=z["off"], nbr=z["nbr"], labels=z["labels"])
+    hq = []
+    for lab, e in zip(z["q_labels"], z["q_edges"]):
+        e = e[e[:, 0] >= 0]
+        hq.append(Graph.from_edges(len(lab), lab, e))
+    rg = gen.make_graph("rmat", 2, scale=12, edge_factor=8, num_labels=32)
+    rq = [(Graph.from_edges(len(e["query"]["labels"]), e["query"]["labels"], e["query"]["edges"]), e["count"])
+          for e in ref["rmat12"]["queries"] if e["count"] is not None]
+    eng = api.Engine(device=local, arena_bytes=args.arena_gb << 30)
+    cases = [(api.DataGraph.from_graph(hg), q, c, 4) for q, c in zip(hq, ref["hprd"])]
+    rdg = api.DataGraph.from_graph(rg)
+    cases += [(rdg, q, c, 12) for q, c in rq]
+    for _ in range(args.warmup):
+        for dg, q, c, mu in cases:
+            api.match_join(eng, dg, q, "CFL_CFL_EXPLORE", max_unit_vertices=mu)
+    dev, wall = 0.0, 0.0
+    for _ in range(args.steps):
+        for dg, q, c, mu in cases:
+            t = time.perf_counter()
+            r = api.match_join(eng, dg, q, "CFL_CFL_EXPLORE", max_unit_vertices=mu)
+            wall += time.perf_counter() - t
+            dev += r.prep_ms + r.enum_ms + r.join_ms
+            if r.count != c:
+                raise SystemExit(f"join count {r.count} differs from the reference's {c}")
+    n = len(cases) * args.steps
+    line = {"metric": "queries/sec (decomposition + hash-join path)", "value": n / (dev / 1e3), "unit": "queries/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "join_hprd_rmat12",
+                       "queries": f"{len(hq)} HPRD-15 (units <= 4 vertices) + {len(rq)} R-MAT scale-12 queries of "
+                                  "16-24 vertices (units <= 12) that the reference's join path finishes",
+                       "method": "CFL_CFL_EXPLORE", "counts": "equal to the reference's -QorCandi Q counts"},
+            "e2e": {"value": n / wall, "unit": "queries/s"}}
+    if args.cpu_baseline and ref_available():
+        tmp = Path(tempfile.mkdtemp(prefix="psmjoin_"))
+        d = tmp / "a" / "b" / "c"
+        (d / "q").mkdir(parents=True)
+        files = {}
+        tot, nref = 0.0, 0
+        for k, (dg, q, c, mu) in enumerate(cases):
+            g = hg if k < len(hq) else rg
+            key = "h" if k < len(hq) else "r"
+            if key not in files:
+                files[key] = d / f"{key}.txt"
+                gen.write_text(g, files[key])
+            qp = d / "q" / f"q{k}.txt"
+            q.write_text(qp)
+            log = tmp / "log.txt"
+            if log.exists():
+                log.unlink()
+            subprocess.run([str(REF_BIN), "-d", str(files[key]), "-q", str(qp), "-num", "MAX", "-time_limit", "120",
+                            "-OutputFile", str(log), "-QorCandi", "Q", "-Qpattern", "STAR", "-JoinMethod", "LEFTDEEP",
+                            "-threadnums", "1", "-BackMethods", "CFL_CFL_EXPLORE"], check=True, capture_output=True,
+                           timeout=300)
+            text = log.read_text()
+            tot += float(re.findall(r"Total time \(seconds\): ([0-9.e+-]+)", text)[-1])
+            nref += 1
+            if tot > args.ref_budget * 4:
+                break
+        line["cpu_baseline"] = {"value": nref / tot, "unit": "queries/s", "cores": 1, "kind": "reference",
+                                "sample": f"{nref} queries through the reference's join path (-QorCandi Q -Qpattern "
+                                          f"STAR -JoinMethod LEFTDEEP -threadnums 1), {tot:.2f} s Total time"}
+    print(json.dumps(line))
+
+
+def serve_leg(args, local):
+    _torch_setup(local)
+    from psm_benchmark_b200 import api, gen
+    nq = args.queries if args.queries != 200 else 5000
+    t = time.time()
+    w = gen.serve(num_queries=nq, scale=args.scale if args.scale != 20 else 24)
+    dg = api.DataGraph.from_graph(w.graph)
+    setup_s = time.time() - t
+    lanes = args.lanes
+    srv = api.Server(dg, w.method, cap=w.cap, time_limit=args.time_limit, lanes=lanes, max_batch=args.max_batch,
+                     lane_arena_bytes=(args.serve_budget_gb << 30) // lanes, full_gpu_lanes=True)
+    # saturation: everything queued at once
+    for q in w.queries[: min(nq, 500)]:
+        srv.submit(q)
+    srv.drain(min(nq, 500))
+    t0 = api.Server.clock_ns()
+    for q in w.queries:
+        srv.submit(q)
+    res = srv.drain(nq, timeout_s=3600)
+    sat = nq / ((max(r.done_ns for r in res) - t0) / 1e9)
+    base = min(r.ticket for r in res)
+    counts = {r.ticket - base: r.count for r in res}
+    loads = {}
+    for load in (0.5, 0.8, 0.95):
+        rate = load * sat
+        arrive = gen.poisson_arrivals(nq, rate, w.seed + int(load * 100))
+        tick0 = None
+        start = api.Server.clock_ns()
+        sched = {}
+        for i, (q, a) in enumerate(zip(w.queries, arrive)):
+            target = start + int(a * 1e9)
+            while api.Server.clock_ns() < target:
+                time.sleep(min(0.0005, max(0.0, (target - api.Server.clock_ns()) / 1e9)))
+            tk = srv.submit(q)
+            tick0 = tk if tick0 is None else tick0
+            sched[tk] = (i, target)
+        out = srv.drain(nq, timeout_s=3600)
+        lat = [(r.done_ns - sched[r.ticket][1]) / 1e6 for r in out]
+        bad = sum(1 for r in out if r.count != counts[sched[r.ticket][0]])
+        span = (max(r.done_ns for r in out) - start) / 1e9
+        loads[f"{int(load * 100)}%"] = {"offered_qps": rate, "achieved_qps": nq / span,
+                                        "p50_ms": float(np.percentile(lat, 50)),
+                                        "p99_ms": float(np.percentile(lat, 99)),
+                                        "mean_batch": float(np.mean([r.batch_size for r in out])),
+                                        "count_mismatches_vs_saturation_run": bad}
+    srv.close()
+    line = {"metric": "queries/sec and p50/p99 latency (serving, continuous batching)", "value": sat,
+            "unit": "queries/s", "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "serve_rmat", "graph": f"R-MAT scale {args.scale if args.scale != 20 else 24}, "
+                                                          "edge factor 16, 128 uniform labels",
+                       "edges": w.graph.num_edges, "queries": nq,
+                       "query_sizes": "{4,8,12,16,24,32} weighted .3/.25/.2/.1/.1/.05", "cap": w.cap,
+                       "lanes": lanes, "max_batch": args.max_batch, "budget_gb": args.serve_budget_gb,
+                       "setup_s": setup_s},
+            "saturation_qps": sat, "loads": loads}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -365,8 +568,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--only", default="", help="comma-separated query indices (profiling runs)")
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "join", "serve"])
+    ap.add_argument("--lanes", type=int, default=1, help="serving lanes")
+    ap.add_argument("--max-batch", type=int, default=512, help="serving batch limit")
+    ap.add_argument("--serve-budget-gb", type=int, default=120, help="serving device-memory budget")
     args = ap.parse_args()
     world, rank, local = dist_setup()
+    if args.workload != "plain":
+        if args.impl == "reference" or world > 1:
+            if rank == 0:
+                print(json.dumps({"impl": args.impl, "unavailable": "the batched, join and serve workloads run on "
+                                                                     "one GPU through this arm only"}))
+            return
+        {"batched": batched_leg, "join": join_leg, "serve": serve_leg}[args.workload](args, dist_setup()[2])
+        return
     if args.impl == "reference":
         reference_arm(args, world, rank)
     else:
