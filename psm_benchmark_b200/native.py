@@ -6,11 +6,13 @@ device, calls raise PsmError.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from functools import lru_cache
 from pathlib import Path
 
 _PKG = Path(__file__).resolve().parent
-LIB_PATH = _PKG / "libpsm_b200.so"
+# PSM_LIB selects another build of the library (A/B timing of kernel variants).
+LIB_PATH = Path(os.environ["PSM_LIB"]) if os.environ.get("PSM_LIB") else _PKG / "libpsm_b200.so"
 
 PSM_OK, PSM_ERR_ARG, PSM_ERR_OOM, PSM_ERR_TIMEOUT, PSM_ERR_CUDA, PSM_ERR_IO, PSM_ERR_INTERNAL = 0, 1, 2, 3, 4, 5, 9
 FILTERS = {"NLF": 0, "GQL": 1, "CFL": 2}
