@@ -9,6 +9,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "host.h"
@@ -75,6 +76,8 @@ struct psm_context {
     int prep_grid_blocks = 0;
     int prep_block_blocks = 0;
     int cluster_size = 0;  // > 0: plain-path preparation by one thread-block cluster of this size
+    int batch_cluster = 0;   // > 0: batched preparation by clusters of this many blocks, one query each
+    int batch_clusters = 0;  // clusters of that launch
     int enum_blocks = 0;
     cudaEvent_t ev[4]{};
     std::vector<char> host_stage;  // QDesc / QState staging
@@ -97,9 +100,12 @@ void psm_context_share_gpu(psm_context* ctx, u32 parts) {
     if (!ctx || parts < 2) return;
     ctx->enum_blocks = std::max(1, ctx->enum_blocks / (int)parts);
     ctx->prep_block_blocks = std::max(1, ctx->prep_block_blocks / (int)parts);
+    ctx->batch_clusters = std::max(1, ctx->batch_clusters / (int)parts);
 }
 
 u64 psm_context_free_bytes(const psm_context* ctx) { return ctx->arena_bytes - ctx->fixed_bytes; }
+
+int psm_context_enum_warps(const psm_context* ctx) { return ctx->enum_blocks * 8; }
 
 int psm_run_internals(psm_run* r, RunInternals* out) {
     if (!r || !r->ctx || !r->d_q) return fail(PSM_ERR_ARG, "run is not alive");
@@ -172,6 +178,10 @@ int setup_query(psm_context* ctx, const psm_graph& g, const QDesc& d, const psm_
     return PSM_OK;
 }
 
+bool use_cluster_batch(const psm_context* ctx, u32 nq) {
+    return ctx->batch_cluster > 0 && nq <= 4u * (u32)ctx->batch_clusters;
+}
+
 u64 budget_ns(const psm_options& o) {
     double s = o.time_limit_s > 0 ? o.time_limit_s : 60.0;
     return (u64)(s * 1e9);
@@ -196,7 +206,8 @@ void fill_result(const DevResult& r, float prep_ms, float enum_ms, u64 donations
 // Runs nq queries. grid_team: prepare the (single) query with the whole grid
 // (plain path); otherwise one block per query (batched path).
 int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, u32 nq, const psm_options& opt,
-                bool grid_team, psm_result* results, psm_run* keep, bool prep_only = false) {
+                bool grid_team, psm_result* results, psm_run* keep, bool prep_only = false, QDoneRec* done = nullptr,
+                u32 exit_keep = 0, void (*poll)(void*) = nullptr, void* poll_arg = nullptr) {
     if (!ctx || !g || !qs || nq == 0) return fail(PSM_ERR_ARG, "null argument");
     if (ctx->run_live) return fail(PSM_ERR_ARG, "a psm_run is still alive on this context");
     CK(cudaSetDevice(ctx->device));
@@ -214,8 +225,13 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     lay.d_enum_q = b.take<char>(psm_enum_query_bytes(nq));
     lay.d_res = b.take<DevResult>(nq);
     if (!lay.d_desc || !lay.d_q || !lay.d_enum_q || !lay.d_res) return fail(PSM_ERR_OOM, "device arena exhausted");
+    // Batched preparation team: a cluster per query while the batch is small
+    // (latency: a query's preparation spreads over the cluster's SMs), a
+    // block per query for large batches (throughput).
+    const bool cluster_batch = !grid_team && use_cluster_batch(ctx, nq);
     // team scans need one word per block of the preparing team (+1)
-    const u32 scan_words = grid_team ? (u32)std::max(ctx->prep_grid_blocks, ctx->cluster_size) + 1 : 2u;
+    const u32 scan_words = grid_team ? (u32)std::max(ctx->prep_grid_blocks, ctx->cluster_size) + 1
+                                     : (cluster_batch ? (u32)ctx->batch_cluster : 1u) + 1;
     std::vector<QState> hq(nq);
     for (u32 i = 0; i < nq; ++i) {
         int rc = setup_query(ctx, *g, descs[i], opt, b, lay.d_desc + i, scan_words, hq[i]);
@@ -242,6 +258,10 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     } else if (grid_team) {
         CK(psm_launch_prep_grid(g->dev, lay.d_q, ctx->d_barrier, ctx->d_devarena, budget, ctx->prep_grid_blocks,
                                 ctx->prep_threads, ctx->st));
+    } else if (cluster_batch) {
+        const int clusters = std::min<int>(ctx->batch_clusters, (int)nq);
+        CK(psm_launch_prep_cluster_batch(g->dev, lay.d_q, nq, ctx->d_ticket, ctx->d_devarena, ctx->batch_cluster,
+                                         clusters, ctx->prep_threads, ctx->st));
     } else {
         int blocks = std::min<int>(ctx->prep_block_blocks, (int)nq);
         CK(psm_launch_prep_block(g->dev, lay.d_q, nq, ctx->d_ticket, ctx->d_devarena, blocks, ctx->prep_threads,
@@ -250,9 +270,19 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     if (!prep_only)
         CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_enum_q, budget, opt.emit ? 1 : 0,
-                           ctx->enum_blocks, ctx->d_enum_cache, ctx->st));
+                           ctx->enum_blocks, ctx->d_enum_cache, done, exit_keep, ctx->st));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     CK(psm_launch_gather(lay.d_q, nq, lay.d_res, ctx->st));
+    if (poll) {
+        // the caller collects per-query completion records while the launch runs
+        cudaError_t q;
+        while ((q = cudaStreamQuery(ctx->st)) == cudaErrorNotReady) {
+            poll(poll_arg);
+            std::this_thread::sleep_for(std::chrono::microseconds(100));
+        }
+        if (q != cudaSuccess) return cuda_fail(q, "batch launch");
+        poll(poll_arg);
+    }
     std::vector<DevResult> res(nq);
     CK(cudaMemcpyAsync(res.data(), lay.d_res, sizeof(DevResult) * nq, cudaMemcpyDeviceToHost, ctx->st));
     EnumStats es{};
@@ -408,6 +438,16 @@ int psm_context_create(int device, uint64_t arena_bytes, psm_context** out) {
         return fail(PSM_ERR_CUDA, "occupancy query failed");
     }
     c->prep_block_blocks = prop.multiProcessorCount * 4;
+    // Batched preparation team: clusters of 8 blocks per query (default), or
+    // one block per query (PSM_BATCH_TEAM=block).
+    const char* bt = getenv("PSM_BATCH_TEAM");
+    if (!(bt && strcmp(bt, "block") == 0)) {
+        int clusters = 0;
+        if (psm_prep_cluster_batch_clusters(c->prep_threads, 8, &clusters) == cudaSuccess && clusters > 0) {
+            c->batch_cluster = 8;
+            c->batch_clusters = clusters;
+        }
+    }
     // PSM_ENUM_CACHE=0 runs the enumerator without prefix-intersection caches.
     const char* ec = getenv("PSM_ENUM_CACHE");
     if (!(ec && strcmp(ec, "0") == 0)) {
@@ -746,7 +786,7 @@ int psm_match_join(psm_context* ctx, const psm_graph* g, const psm_query_desc* q
     std::vector<DevResult> dr(U);
     auto run_units = [&](int emit) -> int {
         CK(psm_launch_enum(g->dev, d_uq, U, ctx->d_enum_scratch, d_enum_q, budget, emit, ctx->enum_blocks,
-                           ctx->d_enum_cache, ctx->st));
+                           ctx->d_enum_cache, nullptr, 0, ctx->st));
         CK(psm_launch_gather(d_uq, U, d_res, ctx->st));
         CK(cudaMemcpyAsync(dr.data(), d_res, sizeof(DevResult) * U, cudaMemcpyDeviceToHost, ctx->st));
         EnumStats es{};
@@ -877,3 +917,12 @@ int psm_hash_join(psm_context* ctx, const uint32_t* r_rows, uint64_t r_n, uint32
 }
 
 }  // extern "C"
+
+int psm_batch_polled(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, u32 nq, const psm_options* opt,
+                     psm_result* results, QDoneRec* done_dev, u32 exit_keep, void (*poll)(void*), void* poll_arg) {
+    if (!opt || !results) return fail(PSM_ERR_ARG, "null argument");
+    return run_queries(ctx, g, qs, nq, *opt, false, results, nullptr, false, done_dev, exit_keep, poll, poll_arg);
+}
+u32 psm_context_prep_blocks_per_query(const psm_context* ctx, u32 nq) {
+    return use_cluster_batch(ctx, nq) ? (u32)ctx->batch_cluster : 1u;
+}

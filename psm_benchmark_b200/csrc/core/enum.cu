@@ -72,6 +72,10 @@ struct EnumCtl {
     u64 donations;
     u64 tasks;
     u64 idle_polls;
+    u32* remaining;     // per query: grabs + donated tasks not yet finished
+    QDoneRec* done;     // per query completion records (host-mapped) or null
+    u32 exit_keep;      // > 0: idle warps beyond this many leave once no work is left
+    u32 pad2;
 };
 
 namespace {
@@ -349,6 +353,19 @@ __device__ __forceinline__ u32 cand_pos(const QState& q, u32 u, u32 v) {
     const u32 word = q.bm[u][b >> 5];
     if (!((word >> (b & 31u)) & 1u)) return 0xFFFFFFFFu;
     return q.rank[u][b >> 5] + __popc(word & ((1u << (b & 31u)) - 1u));
+}
+
+// Writes a finished query's completion record (its count is final: every
+// task of the query published before the caller's counter reached zero).
+__device__ void finish_query(QState& q, QDoneRec* rec) {
+    __threadfence();
+    const u64 c = atomicAdd((unsigned long long*)&q.count, 0ull);
+    rec->count = q.cap && c > q.cap ? q.cap : c;
+    rec->overtime = ld_volatile_u32(&q.overtime);
+    rec->status = q.status;
+    rec->done_ns = global_timer_ns();
+    __threadfence_system();
+    *(volatile u32*)&rec->flag = 1u;
 }
 
 // Marks the query stopped (cap reached); the first caller stamps the time.
@@ -776,7 +793,10 @@ __device__ bool try_donate_range(EnumCtl* ctl, Slot* slots, u32 kind, u32 qi, u3
     const u32 lane = lane_id();
     const u32 mid = cur + ((end - cur) >> 1);
     TaskHdr h{kind, qi, d0, mid, end, drv};
-    if (lane == 0) atomicAdd(&ctl->pending, 1ull);
+    if (lane == 0) {
+        atomicAdd(&ctl->pending, 1ull);
+        atomicAdd(&ctl->remaining[qi], 1u);
+    }
     __threadfence();
     __syncwarp();
     if (enqueue(ctl, slots, h, ws, d0, 0xFFFFFFFFu, 0)) {
@@ -784,7 +804,10 @@ __device__ bool try_donate_range(EnumCtl* ctl, Slot* slots, u32 kind, u32 qi, u3
         end = mid;
         return true;
     }
-    if (lane == 0) atomicAdd(&ctl->pending, (unsigned long long)-1ll);
+    if (lane == 0) {
+        atomicSub(&ctl->remaining[qi], 1u);  // the donor's own task still holds the query open
+        atomicAdd(&ctl->pending, (unsigned long long)-1ll);
+    }
     return false;
 }
 
@@ -817,7 +840,10 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
             const u32 qlen = warp_ld_volatile_u32(&ctl->q_tail) - warp_ld_volatile_u32(&ctl->q_head);
             if (de < d && qlen < hungry) {
                 TaskHdr h{KIND_FULL, qi, de + 1, 0, 0, 0};
-                if (lane == 0) atomicAdd(&ctl->pending, 1ull);
+                if (lane == 0) {
+                    atomicAdd(&ctl->pending, 1ull);
+                    atomicAdd(&ctl->remaining[qi], 1u);
+                }
                 __threadfence();
                 __syncwarp();
                 if (enqueue(ctl, slots, h, ws, de, de, ws->chunk[de][ws->cn[de] - 1])) {
@@ -827,6 +853,7 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
                         atomicAdd((unsigned long long*)&ctl->donations, 1ull);
                     }
                 } else if (lane == 0) {
+                    atomicSub(&ctl->remaining[qi], 1u);
                     atomicAdd(&ctl->pending, (unsigned long long)-1ll);
                 }
                 __syncwarp();
@@ -1155,6 +1182,8 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 4) enum_kernel(DevGraph 
             __syncwarp();
             if (lane == 0) {
                 __threadfence();
+                // the query's last task publishes its result
+                if (atomicSub(&ctl->remaining[t.qi], 1u) == 1u && ctl->done) finish_query(qs[t.qi], ctl->done + t.qi);
                 atomicAdd(&ctl->pending, (unsigned long long)-1ll);
             }
             continue;
@@ -1165,6 +1194,20 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 4) enum_kernel(DevGraph 
         if (lane == 0) pend = ld_acquire_u64((const u64*)&ctl->pending);
         pend = __shfl_sync(FULL_MASK, pend, 0);
         if (pend == 0) break;
+        if (ctl->exit_keep && warp_ld_volatile_u32(&ctl->ticket) >= ctl->total_grabs &&
+            warp_ld_volatile_u32(&ctl->q_tail) == warp_ld_volatile_u32(&ctl->q_head)) {
+            // nothing to take: leave (freeing the SM for other launches)
+            // while more than exit_keep warps stay to take donations
+            u32 leave = 0;
+            if (lane == 0) {
+                const u32 old = atomicSub(&ctl->hungry, 1u);
+                if (old > ctl->exit_keep)
+                    leave = 1;
+                else
+                    atomicAdd(&ctl->hungry, 1u);
+            }
+            if (__shfl_sync(FULL_MASK, leave, 0)) break;
+        }
         ++spins;
         ++npolls;
         if ((spins & 255u) == 0) {
@@ -1185,9 +1228,9 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 4) enum_kernel(DevGraph 
 
 // Single block: per-query initial pools (edges of the first table for
 // queries of four or more vertices, roots otherwise), their prefix in grabs,
-// and the queue's sequence numbers.
+// the per-query task counts and the queue's sequence numbers.
 __global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, u32* grab_prefix, PoolInfo* pools,
-                                 u32 total_warps, u64 budget_ns) {
+                                 u32* remaining, QDoneRec* done, u32 exit_keep, u32 total_warps, u64 budget_ns) {
     __shared__ u32 s_carry;
     __shared__ u32 wt[32];
     if (threadIdx.x == 0) s_carry = 0;
@@ -1218,6 +1261,8 @@ __global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, 
                 grabs = (pi.units + pi.grab - 1) / pi.grab;
             }
             pools[i] = pi;
+            remaining[i] = grabs;
+            if (grabs == 0 && done) finish_query(qs[i], done + i);  // nothing to enumerate
         }
         u32 incl = warp_incl_scan(grabs);
         if (lane_id() == 31) wt[threadIdx.x >> 5] = incl;
@@ -1248,6 +1293,9 @@ __global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, 
         ctl->donations = 0;
         ctl->tasks = 0;
         ctl->idle_polls = 0;
+        ctl->remaining = remaining;
+        ctl->done = done;
+        ctl->exit_keep = exit_keep;
     }
     for (u32 i = threadIdx.x; i < QCAP; i += blockDim.x) slots[i].seq = i;
 }
@@ -1287,17 +1335,20 @@ size_t psm_enum_cache_bytes(int blocks) {
     return (size_t)blocks * WARPS_PER_BLOCK * PSM_MAXQ * SLOT_WORDS * sizeof(u32);
 }
 
-// Per-query scratch of the enumeration: grab prefix (nq + 1 words) and pool
-// descriptors.
-size_t psm_enum_query_bytes(u32 nq) { return align16(sizeof(u32) * (nq + 1)) + sizeof(PoolInfo) * nq; }
+// Per-query scratch of the enumeration: grab prefix (nq + 1 words), pool
+// descriptors and remaining-task counts.
+size_t psm_enum_query_bytes(u32 nq) {
+    return align16(sizeof(u32) * (nq + 1)) + align16(sizeof(PoolInfo) * nq) + sizeof(u32) * nq;
+}
 
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
-                            int emit, int blocks, u32* cache, cudaStream_t st) {
+                            int emit, int blocks, u32* cache, QDoneRec* done, u32 exit_keep, cudaStream_t st) {
     EnumCtl* ctl = (EnumCtl*)scratch;
     Slot* slots = (Slot*)((char*)scratch + align16(sizeof(EnumCtl)));
     u32* grab_prefix = (u32*)query_scratch;
     PoolInfo* pools = (PoolInfo*)((char*)query_scratch + align16(sizeof(u32) * (nq + 1)));
-    enum_init_kernel<<<1, 1024, 0, st>>>(qs, nq, ctl, slots, grab_prefix, pools,
+    u32* remaining = (u32*)((char*)pools + align16(sizeof(PoolInfo) * nq));
+    enum_init_kernel<<<1, 1024, 0, st>>>(qs, nq, ctl, slots, grab_prefix, pools, remaining, done, exit_keep,
                                          (u32)blocks * WARPS_PER_BLOCK, budget_ns);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

@@ -54,6 +54,16 @@ int psm_run_internals(psm_run* run, RunInternals* out);
 void psm_context_share_gpu(psm_context* ctx, u32 parts);
 // Arena bytes available to a batch (the arena minus its fixed region).
 u64 psm_context_free_bytes(const psm_context* ctx);
+// Warps of the context's enumeration launches.
+int psm_context_enum_warps(const psm_context* ctx);
+// Blocks that prepare one query of a batch of nq queries.
+u32 psm_context_prep_blocks_per_query(const psm_context* ctx, u32 nq);
+// Batched path with per-query completion: the enumerator writes a QDoneRec
+// per query into done_dev (device address of host-mapped memory) as each
+// query finishes, and poll(poll_arg) runs every 0.1 ms until the launch
+// ends. exit_keep > 0 lets idle warps leave once no work is left.
+int psm_batch_polled(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, u32 nq, const psm_options* opt,
+                     psm_result* results, QDoneRec* done_dev, u32 exit_keep, void (*poll)(void*), void* poll_arg);
 
 // Builds the device query descriptor (validation, NLF lists, CFL plans).
 // Returns PSM_OK or PSM_ERR_ARG with *err set.
@@ -68,6 +78,9 @@ cudaError_t psm_launch_prep_block(const DevGraph& g, QState* qs, u32 nq, u32* ti
 cudaError_t psm_launch_prep_grid(const DevGraph& g, QState* qs, void* barrier, DevArena* arena, u64 budget_ns,
                                  int blocks, int threads, cudaStream_t st);
 cudaError_t psm_prep_grid_max_blocks(int threads, int* blocks);
+cudaError_t psm_prep_cluster_batch_clusters(int threads, int cluster, int* clusters);
+cudaError_t psm_launch_prep_cluster_batch(const DevGraph& g, QState* qs, u32 nq, u32* ticket, DevArena* arena,
+                                          int cluster, int clusters, int threads, cudaStream_t st);
 cudaError_t psm_prep_cluster_size(int threads, int want, int* size);
 cudaError_t psm_launch_prep_cluster(const DevGraph& g, QState* qs, DevArena* arena, int cluster, int threads,
                                     cudaStream_t st);
@@ -75,9 +88,11 @@ size_t psm_enum_scratch_bytes();
 size_t psm_enum_query_bytes(u32 nq);
 size_t psm_enum_cache_bytes(int blocks);
 // cache: psm_enum_cache_bytes(blocks) of device memory for the per-warp
-// prefix-intersection caches, or null to run without them.
+// prefix-intersection caches, or null to run without them. done: per-query
+// completion records in host-mapped memory (device address), or null.
+// exit_keep > 0 lets idle warps beyond that many leave once no work is left.
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
-                            int emit, int blocks, u32* cache, cudaStream_t st);
+                            int emit, int blocks, u32* cache, QDoneRec* done, u32 exit_keep, cudaStream_t st);
 cudaError_t psm_enum_max_blocks(int* blocks);
 cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st);
 cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st);

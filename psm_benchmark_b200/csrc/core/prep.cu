@@ -1254,6 +1254,24 @@ __global__ void __launch_bounds__(512) prep_block_kernel(DevGraph g, QState* qs,
     }
 }
 
+// Batched path with cluster teams: each thread-block cluster takes the next
+// query from a ticket (read by block 0, handed to the others through
+// distributed shared memory) and prepares it with all of its blocks.
+__global__ void __launch_bounds__(512) prep_cluster_batch_kernel(DevGraph g, QState* qs, u32 nq, u32* ticket,
+                                                                 DevArena* arena) {
+    __shared__ u32 s_q;
+    ClusterTeam t;
+    cg::cluster_group cl = cg::this_cluster();
+    while (true) {
+        if (cl.block_rank() == 0 && threadIdx.x == 0) s_q = atomicAdd(ticket, 1u);
+        cl.sync();
+        const u32 qi = *cl.map_shared_rank(&s_q, 0);
+        cl.sync();  // every block has read it before block 0 takes the next
+        if (qi >= nq) break;
+        prepare_query(t, g, qs[qi], arena);
+    }
+}
+
 // Plain path: one query prepared by one thread-block cluster.
 __global__ void __launch_bounds__(512) prep_cluster_kernel(DevGraph g, QState* qs, DevArena* arena) {
     ClusterTeam t;
@@ -1328,6 +1346,44 @@ cudaError_t psm_launch_prep_cluster(const DevGraph& g, QState* qs, DevArena* are
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, prep_cluster_kernel, g, qs, arena);
+}
+
+// Clusters of `cluster` blocks that fit the GPU at once for the batched
+// cluster preparation kernel (0 if that cluster size cannot run).
+cudaError_t psm_prep_cluster_batch_clusters(int threads, int cluster, int* clusters) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cluster);
+    cfg.blockDim = dim3(threads);
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    *clusters = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(clusters, prep_cluster_batch_kernel, &cfg);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *clusters = 0;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t psm_launch_prep_cluster_batch(const DevGraph& g, QState* qs, u32 nq, u32* ticket, DevArena* arena,
+                                          int cluster, int clusters, int threads, cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(cluster * clusters);
+    cfg.blockDim = dim3(threads);
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, prep_cluster_batch_kernel, g, qs, nq, ticket, arena);
 }
 
 cudaError_t psm_prep_grid_max_blocks(int threads, int* blocks) {

@@ -181,6 +181,18 @@ struct DevResult {
     u32 status, overtime, filter_ok, empty;
 };
 
+// Completion record of one query of an enumeration launch, written by the
+// enumerator into host-mapped memory as soon as the query's last task ends
+// (serving: results leave before the rest of their batch).
+struct QDoneRec {
+    u64 count;     // min(count, cap)
+    u64 done_ns;   // %globaltimer at completion
+    u32 overtime;
+    u32 status;    // PSM_DEV_* of the query's preparation
+    u32 flag;      // set last: 1 once the record is complete
+    u32 pad;
+};
+
 // Launch-wide counters of the enumeration scheduler, read back by the host.
 struct EnumStats {
     u32 error;

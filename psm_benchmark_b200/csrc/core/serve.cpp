@@ -14,7 +14,12 @@
 // launch (a block per query) and one persistent enumeration launch. Requests
 // that arrive while other lanes' batches are on the GPU are admitted by the
 // next lane that frees up, so the work of several batches overlaps on the
-// device. A batch whose tables outgrow the estimate is rerun query by query.
+// device. Each query's result leaves as soon as its own last enumeration task
+// ends: the enumerator writes a completion record into host-mapped memory,
+// which the lane thread polls while its batch runs; with several lanes, idle
+// warps of a batch leave the GPU once no work is left so that the next
+// batch's launches get the SMs. A batch whose tables outgrow the estimate is
+// rerun query by query.
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -47,13 +52,20 @@ struct Request {
 
 }  // namespace
 
+struct Lane {
+    psm_context* ctx = nullptr;
+    QDoneRec* rec_host = nullptr;  // host-mapped completion records [max_batch]
+    QDoneRec* rec_dev = nullptr;
+};
+
 struct psm_server {
     int device = 0;
     const psm_graph* g = nullptr;
     psm_options opt{};
     psm_server_config cfg{};
     u64 budget = 0;  // admission budget per lane (arena bytes minus the fixed region)
-    std::vector<psm_context*> ctx;
+    u32 prep_blocks = 1;  // largest number of blocks that prepare one query
+    std::vector<Lane> lanes;
     std::vector<std::thread> threads;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
@@ -66,8 +78,9 @@ struct psm_server {
 
 namespace {
 
-// Device bytes a query takes in a batch (see the file comment).
-u64 estimate_bytes(const psm_graph& g, const psm_query_desc& q) {
+// Device bytes a query takes in a batch (see the file comment); prep_blocks:
+// blocks preparing one query (each keeps its own CFL path-estimate buffers).
+u64 estimate_bytes(const psm_graph& g, const psm_query_desc& q, const psm_options& opt, u32 prep_blocks) {
     const u32 n = q.num_vertices;
     u64 b = al(sizeof(QState)) + al(sizeof(QDesc)) + al(sizeof(DevResult)) + 64;
     u64 maxw = 1, maxb = 1, rows = 0;
@@ -83,7 +96,8 @@ u64 estimate_bytes(const psm_graph& g, const psm_query_desc& q) {
         maxb = std::max(maxb, B);
         rows += B * deg[u];
     }
-    b += 2 * al(4 * maxw) + al(4 * (rows + 1)) + al(8) + al(8ull * 2 * 64 * maxb) + al(8ull * PSM_PLAN_WORDS);
+    b += 2 * al(4 * maxw) + al(4 * (rows + 1)) + al(8ull * (prep_blocks + 1));
+    if (opt.order == PSM_ORDER_CFL) b += al(8ull * 2 * prep_blocks * maxb) + al(8ull * PSM_PLAN_WORDS);
     for (u32 e = 0; e < q.num_edges; ++e) {
         const u32 la = q.labels[q.edges[2 * e]], lb = q.labels[q.edges[2 * e + 1]];
         b += 4 * (g.pair_edges(la, lb) + g.pair_edges(lb, la));
@@ -107,9 +121,47 @@ void finish(psm_server* s, const Request& r, const psm_result& res, int status, 
     s->done.push_back(o);
 }
 
+// Poll state of a lane's running batch.
+struct Inflight {
+    psm_server* s;
+    Lane* ln;
+    std::vector<Request>* batch;
+    std::vector<char> sent;
+    u64 t0;
+    u32 lane;
+    u32 base;  // first record of this (sub)batch
+    u32 n;
+};
+
+void poll_records(void* arg) {
+    auto* f = (Inflight*)arg;
+    std::vector<u32> fresh;
+    for (u32 i = 0; i < f->n; ++i) {
+        if (f->sent[f->base + i]) continue;
+        // a query whose preparation failed is reported from the batch's results
+        if (*(volatile u32*)&f->ln->rec_host[i].flag && f->ln->rec_host[i].status == PSM_DEV_OK) fresh.push_back(i);
+    }
+    if (fresh.empty()) return;
+    std::atomic_thread_fence(std::memory_order_acquire);  // record fields after their flag
+    const u64 t1 = now_ns();
+    std::lock_guard<std::mutex> lk(f->s->mu);
+    for (u32 i : fresh) {
+        const QDoneRec& r = f->ln->rec_host[i];
+        psm_result res{};
+        res.count = r.count;
+        res.overtime = r.overtime;
+        finish(f->s, (*f->batch)[f->base + i], res, r.overtime ? PSM_ERR_TIMEOUT : PSM_OK, f->t0, t1,
+               (u32)f->n, f->lane);
+        f->sent[f->base + i] = 1;
+    }
+    f->s->cv_done.notify_all();
+}
+
 void lane_loop(psm_server* s, u32 lane) {
     cudaSetDevice(s->device);
-    psm_context* ctx = s->ctx[lane];
+    Lane& ln = s->lanes[lane];
+    psm_context* ctx = ln.ctx;
+    const u32 keep = s->cfg.lanes > 1 ? (u32)std::max(8, psm_context_enum_warps(ctx) / 16) : 0u;
     for (;;) {
         std::vector<Request> batch;
         {
@@ -140,11 +192,20 @@ void lane_loop(psm_server* s, u32 lane) {
             qs[i] = psm_query_desc{(u32)batch[i].labels.size(), (u32)(batch[i].edges.size() / 2),
                                    batch[i].labels.data(), batch[i].edges.data()};
         std::vector<psm_result> res(batch.size());
-        int rc = psm_match_batch(ctx, s->g, qs.data(), (u32)qs.size(), &s->opt, res.data());
+        Inflight f{s, &ln, &batch, std::vector<char>(batch.size(), 0), t0, lane, 0, (u32)batch.size()};
+        memset(ln.rec_host, 0, sizeof(QDoneRec) * batch.size());
+        int rc = psm_batch_polled(ctx, s->g, qs.data(), (u32)qs.size(), &s->opt, res.data(), ln.rec_dev, keep,
+                                  poll_records, &f);
         std::vector<int> st(batch.size(), rc);
         if (rc == PSM_ERR_OOM && batch.size() > 1) {
             // the tables outgrew the estimate: one query at a time
-            for (size_t i = 0; i < batch.size(); ++i) st[i] = psm_match_batch(ctx, s->g, &qs[i], 1, &s->opt, &res[i]);
+            for (size_t i = 0; i < batch.size(); ++i) {
+                if (f.sent[i]) continue;
+                memset(ln.rec_host, 0, sizeof(QDoneRec));
+                f.base = (u32)i;
+                f.n = 1;
+                st[i] = psm_batch_polled(ctx, s->g, &qs[i], 1, &s->opt, &res[i], ln.rec_dev, keep, poll_records, &f);
+            }
         } else if (rc == PSM_OK || rc == PSM_ERR_TIMEOUT) {
             for (size_t i = 0; i < batch.size(); ++i) st[i] = (int)res[i].status;
         }
@@ -152,7 +213,7 @@ void lane_loop(psm_server* s, u32 lane) {
         {
             std::lock_guard<std::mutex> lk(s->mu);
             for (size_t i = 0; i < batch.size(); ++i)
-                finish(s, batch[i], res[i], st[i], t0, t1, (u32)batch.size(), lane);
+                if (!f.sent[i]) finish(s, batch[i], res[i], st[i], t0, t1, (u32)batch.size(), lane);
             s->running -= batch.size();
         }
         s->cv_done.notify_all();
@@ -173,18 +234,32 @@ int psm_server_create(int device, const psm_graph* g, const psm_options* opt, co
     s->g = g;
     s->opt = *opt;
     s->cfg = *cfg;
+    auto cleanup = [&]() {
+        for (auto& x : s->lanes) {
+            if (x.ctx) psm_context_free(x.ctx);
+            if (x.rec_host) cudaFreeHost(x.rec_host);
+        }
+        delete s;
+    };
     for (u32 l = 0; l < cfg->lanes; ++l) {
-        psm_context* c = nullptr;
-        int rc = psm_context_create(device, cfg->lane_arena_bytes, &c);
+        Lane ln;
+        int rc = psm_context_create(device, cfg->lane_arena_bytes, &ln.ctx);
         if (rc) {
-            for (auto* x : s->ctx) psm_context_free(x);
-            delete s;
+            cleanup();
             return rc;
         }
-        if (cfg->lanes > 1 && !cfg->full_gpu_lanes) psm_context_share_gpu(c, cfg->lanes);
-        s->ctx.push_back(c);
+        if (cfg->lanes > 1 && !cfg->full_gpu_lanes) psm_context_share_gpu(ln.ctx, cfg->lanes);
+        cudaError_t e = cudaHostAlloc((void**)&ln.rec_host, sizeof(QDoneRec) * cfg->max_batch,
+                                      cudaHostAllocMapped | cudaHostAllocPortable);
+        if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&ln.rec_dev, ln.rec_host, 0);
+        s->lanes.push_back(ln);
+        if (e != cudaSuccess) {
+            cleanup();
+            return psm_fail(PSM_ERR_CUDA, std::string("completion records: ") + cudaGetErrorString(e));
+        }
     }
-    s->budget = psm_context_free_bytes(s->ctx[0]);
+    s->budget = psm_context_free_bytes(s->lanes[0].ctx);
+    s->prep_blocks = psm_context_prep_blocks_per_query(s->lanes[0].ctx, 1);
     for (u32 l = 0; l < cfg->lanes; ++l) s->threads.emplace_back(lane_loop, s, l);
     *out = s;
     return PSM_OK;
@@ -199,7 +274,7 @@ int psm_server_submit(psm_server* s, const psm_query_desc* q, uint64_t* ticket) 
     r.edges.assign(q->edges, q->edges + 2ull * q->num_edges);
     for (u32 x : r.edges)
         if (x >= q->num_vertices) return psm_fail(PSM_ERR_ARG, "edge endpoint out of range");
-    r.est = estimate_bytes(*s->g, *q);
+    r.est = estimate_bytes(*s->g, *q, s->opt, s->prep_blocks);
     r.submit_ns = now_ns();
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -233,7 +308,7 @@ int psm_server_pending(psm_server* s, uint64_t* queued, uint64_t* running) {
 
 int psm_server_estimate(psm_server* s, const psm_query_desc* q, uint64_t* bytes, uint64_t* lane_budget) {
     if (!s || !q || !bytes) return psm_fail(PSM_ERR_ARG, "null argument");
-    *bytes = estimate_bytes(*s->g, *q);
+    *bytes = estimate_bytes(*s->g, *q, s->opt, s->prep_blocks);
     if (lane_budget) *lane_budget = s->budget;
     return PSM_OK;
 }
@@ -248,7 +323,10 @@ void psm_server_destroy(psm_server* s) {
     }
     s->cv_work.notify_all();
     for (auto& t : s->threads) t.join();
-    for (auto* c : s->ctx) psm_context_free(c);
+    for (auto& ln : s->lanes) {
+        psm_context_free(ln.ctx);
+        cudaFreeHost(ln.rec_host);
+    }
     delete s;
 }
 
