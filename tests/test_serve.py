@@ -66,7 +66,7 @@ def test_admission_refuses_requests_beyond_the_budget(engine):
     qs = gen.make_queries(g0, [3, 12], gen.BASE_SEED + 11)
     dg = api.DataGraph.from_graph(g0)
     with api.Server(dg, "GQL_GQL_GQL", cap=1000, time_limit=60, lanes=1, max_batch=4,
-                    lane_arena_bytes=8 << 20) as srv:
+                    lane_arena_bytes=64 << 20) as srv:
         small, budget = srv.estimate(qs[0])
         big, _ = srv.estimate(qs[1])
         assert small <= budget < big
