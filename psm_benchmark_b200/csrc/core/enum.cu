@@ -96,6 +96,7 @@ enum : u32 {
 constexpr u32 CACHE_CAP = 512;
 constexpr u32 BM_WORDS = PSM_CACHE_BM_BITS / 32;
 constexpr u32 SLOT_WORDS = CACHE_CAP + BM_WORDS;
+constexpr u32 WARP_CACHE_WORDS = PSM_MAXQ * SLOT_WORDS + PSM_MEMO_CAP;  // slots + weight memo
 constexpr u32 NO_ROW = 0xFFFFFFFFu;
 constexpr u32 LONG_ROW = 24;     // per-lane binary-search walks longer than this go to the warp
 constexpr u32 LONG_BM_ROW = 96;  // per-lane bitmap walks longer than this go to the warp
@@ -108,6 +109,10 @@ constexpr u32 LONG_BM_ROW = 96;  // per-lane bitmap walks longer than this go to
 // bitmaps start each task (and each launch) empty.
 struct WarpStack {
     u32* cbuf;          // this warp's slots (null: caching off)
+    u32* memo;          // this warp's weight memo [PSM_MEMO_CAP] (entries w + 1; 0 = not known)
+    u64 rsum;           // memo: total length of the depth-l rows of S_d's candidates (valid with rsum_ok)
+    u32 rsum_ok;
+    u32 lvfull;         // depths whose driver range is the whole level (not a donated part)
     u32 cvalid;
     u32 cover;          // depths whose intersection overflowed CACHE_CAP for the current prefix
     u32 cbits;
@@ -265,6 +270,14 @@ __device__ bool ensure_cache(const QState& q, u32 d, WarpStack* ws, u64& bytes) 
         __syncwarp();
     }
     if (!over && ((q.bm_depths >> d) & 1u)) set_bits(q, ws, d);
+    if (q.memo_ok && d + 2 == q.n_enum) {
+        // the weight memo belongs to S_d: start it afresh
+        const u32 nl = q.cnt[q.order[d + 1]];
+        for (u32 i = lane; i < nl; i += 32) ws->memo[i] = 0u;
+        __syncwarp();
+        if (lane == 0) ws->rsum_ok = 0;
+        __syncwarp();
+    }
     if (lane == 0) {
         if (over)
             ws->cover |= bit;
@@ -330,6 +343,7 @@ __device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws
         ws->ohi[d] = ohi;
         ws->cn[d] = 0;
         ws->ci[d] = 0;
+        ws->lvfull |= 1u << d;
     }
     __syncwarp();
     return dhi - dlo;
@@ -685,6 +699,93 @@ __device__ u64 warp_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
     return c;
 }
 
+// Completions of every candidate of depth d (= n-2, whose candidate set is
+// its cache S_d, a whole level) at depth l = d + 1 given the prefix, through
+// the weight memo (QState::memo_ok):
+//   sum over p in S_d \ U, x in S_l \ V of [x in R(p)]
+//     = sum_{x in S_l \ V} w(x) - sum_{u in U ∩ S_d} |R(u) ∩ S_l \ V|,
+// with w(x) = |T[u_l -> u_d][x] ∩ S_d| (memoised), R(p) = T[u_d -> u_l][p],
+// U / V the data vertices used by earlier same-label depths of u_d / u_l
+// (p's own vertex is never in R(p): no self loops). Warp-uniform. Adds the
+// reference-equivalent bytes of the level's last-depth intersections.
+struct MemoOut {
+    u64 count, bytes, calls;
+};
+
+__device__ __forceinline__ MemoOut memo_count(const QState& q, u32 d, WarpStack* ws) {
+    const u32 lane = lane_id();
+    const u32 l = d + 1;
+    const u32 ud = q.order[d], ul = q.order[l];
+    const u32* Sd = cache_list(q, ws, d);
+    const u32 sd = ws->clen[d];
+    const u32* bmd = slot_bm(ws, d);
+    const u32* Sl = cache_list(q, ws, l);
+    const u32 sl = ws->clen[l];
+    const u32* list_l = q.list[ul];
+    const u32 rbase = q.bn_tab[l][q.crow[l]];  // rows R(p) of T[u_d -> u_l]
+    const u32 umask = q.same_mask[d];
+    const u32 vmask = q.same_mask[l] & ~(1u << d);
+    u32* memo = ws->memo;
+    auto in_v = [&](u32 y) {
+        if (!vmask) return false;
+        const u32 vy = list_l[y];
+        for (u32 m = vmask; m; m &= m - 1)
+            if (ws->vid[__ffs(m) - 1] == vy) return true;
+        return false;
+    };
+    // sum of w(x) over S_l \ V
+    u64 a = 0;
+    for (u32 i = lane; i < sl; i += 32) {
+        const u32 x = Sl[i];
+        if (in_v(x)) continue;
+        u32 e = memo[x];
+        if (e == 0) {
+            const u32 lo = q.P[q.memo_tab + x], hi = q.P[q.memo_tab + x + 1];
+            u32 w = 0;
+            for (u32 k = lo; k < hi; ++k) w += bm_test(bmd, __ldg(q.adj + k));
+            e = w + 1;
+            memo[x] = e;
+        }
+        a += e - 1;
+    }
+    // used same-label vertices among S_d: their completions and their rows
+    u64 b = 0, ru = 0, nu = 0;
+    if ((umask >> lane) & 1u) {
+        const u32 pu = cand_pos(q, ud, ws->vid[lane]);
+        if (pu != 0xFFFFFFFFu && bm_test(bmd, pu)) {
+            const u32 lo = q.P[rbase + pu], hi = q.P[rbase + pu + 1];
+            for (u32 k = lo; k < hi; ++k) {
+                const u32 y = __ldg(q.adj + k);
+                b += in_cache(q, ws, l, y) && !in_v(y);
+            }
+            ru = hi - lo;
+            nu = 1;
+        }
+    }
+    // reference-equivalent bytes: each accepted p of depth d intersects all
+    // of depth l's rows
+    if (!ws->rsum_ok) {
+        u64 rs = 0;
+        for (u32 i = lane; i < sd; i += 32) {
+            const u32 p = Sd[i];
+            rs += q.P[rbase + p + 1] - q.P[rbase + p];
+        }
+        rs = warp_sum64(rs);
+        __syncwarp();
+        if (lane == 0) {
+            ws->rsum = rs;
+            ws->rsum_ok = 1;
+        }
+        __syncwarp();
+    }
+    a = warp_sum64(a);
+    b = warp_sum64(b);
+    ru = warp_sum64(ru);
+    nu = warp_sum64(nu);
+    const u64 accepted = sd - nu;
+    return MemoOut{a - b, accepted * (8ull * q.nbn[l] + 4ull * ws->csum[l]) + 4ull * (ws->rsum - ru), accepted};
+}
+
 // ---------------------------------------------------------------- queue --
 
 // Bounded lock-free MPMC ring with a sequence number per slot. Lane 0 claims
@@ -830,7 +931,10 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
             bool done = try_donate_range(ctl, slots, KIND_RANGE, qi, dd, ws->cur[dd], end,
                                          ws->drv[dd] | (ws->flg[dd] << 16), ws, 64u);
             __syncwarp();
-            if (done && lane == 0) ws->end[dd] = end;
+            if (done && lane == 0) {
+                ws->end[dd] = end;
+                ws->lvfull &= ~(1u << dd);
+            }
             __syncwarp();
         } else {
             u32 de = d0;
@@ -890,6 +994,22 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
         if (d + 2 == n && !emit) {
             // The last two depths fused: each lane takes one driver element
             // of depth d and counts its completions at depth d + 1 on its own.
+            if (ws->cur[d] < ws->end[d] && q.memo_ok && ((ws->lvfull >> d) & 1u) &&
+                (ws->flg[d] & LV_CACHED) && ((ws->cbits >> d) & 1u) && ensure_cache(q, d + 1, ws, bytes)) {
+                // the whole level at once through the weight memo
+                const MemoOut mo = memo_count(q, d, ws);
+                count += mo.count;
+                bytes += mo.bytes;
+                calls += mo.calls;
+                __syncwarp();
+                if (lane == 0) ws->cur[d] = ws->end[d];
+                __syncwarp();
+                if ((++iter & 15u) == 0 && periodic(q, qi, ws, d, d0, iter, count, ctl, slots)) {
+                    go = false;
+                    break;
+                }
+                continue;
+            }
             if (ws->cur[d] < ws->end[d]) {
                 const u32 cur = ws->cur[d], end = ws->end[d];
                 const u32 idx = cur + lane;
@@ -1089,6 +1209,7 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
             }
             __syncwarp();
             if (lane == 0) {
+                ws->lvfull &= ~(1u << d0);  // a part of the donor's level
                 ws->flg[d0] = flg;
                 ws->cur[d0] = t.b;
                 ws->end[d0] = t.e;
@@ -1152,7 +1273,7 @@ __device__ bool take_initial(EnumCtl* ctl, const u32* grab_prefix, const PoolInf
     return true;
 }
 
-__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 4) enum_kernel(DevGraph g, QState* qs, EnumCtl* ctl,
+__global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 3) enum_kernel(DevGraph g, QState* qs, EnumCtl* ctl,
                                                                     Slot* slots, const u32* grab_prefix,
                                                                     const PoolInfo* pools, int emit, u32* cache) {
     __shared__ WarpStack stacks[WARPS_PER_BLOCK];
@@ -1160,7 +1281,10 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 4) enum_kernel(DevGraph 
     const u32 lane = lane_id();
     if (lane == 0) {
         const size_t warp = (size_t)blockIdx.x * WARPS_PER_BLOCK + (threadIdx.x >> 5);
-        ws->cbuf = cache ? cache + warp * (PSM_MAXQ * SLOT_WORDS) : nullptr;
+        ws->cbuf = cache ? cache + warp * WARP_CACHE_WORDS : nullptr;
+        ws->memo = cache ? ws->cbuf + PSM_MAXQ * SLOT_WORDS : nullptr;
+        ws->rsum_ok = 0;
+        ws->lvfull = 0;
         ws->cvalid = 0;
         ws->cover = 0;
         ws->cbits = 0;
@@ -1332,7 +1456,7 @@ size_t psm_enum_scratch_bytes() { return align16(sizeof(EnumCtl)) + sizeof(Slot)
 
 // Per-warp prefix-intersection caches of a launch of `blocks` blocks.
 size_t psm_enum_cache_bytes(int blocks) {
-    return (size_t)blocks * WARPS_PER_BLOCK * PSM_MAXQ * SLOT_WORDS * sizeof(u32);
+    return (size_t)blocks * WARPS_PER_BLOCK * WARP_CACHE_WORDS * sizeof(u32);
 }
 
 // Per-query scratch of the enumeration: grab prefix (nq + 1 words), pool

@@ -908,9 +908,21 @@ __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
     }
     const bool bm_ok = act && q.cnt[u] <= PSM_CACHE_BM_BITS;
     const u32 bm_depths = __ballot_sync(FULL_MASK, bm_ok);
+    const u32 cm_all = cm;
     // one shallow row is worth caching only as a bitmap tested against the
     // depth-(d-1) row
     if (__popc(cm) < 2 && !(__popc(cm) == 1 && crow != 0xFFFFFFFFu && bm_ok)) cm = 0;
+    // last-two-depth weight memo (see QState::memo_ok): depth n-1 has a cache
+    // and a row at depth n-2; depth n-2 has rows at depths <= n-4 only, all
+    // kept in its cache (even a single one) with a bitmap
+    const u32 last = n >= 3 ? n - 1 : 0u;
+    const u32 cm_l = __shfl_sync(FULL_MASK, cm, last), crow_l = __shfl_sync(FULL_MASK, crow, last);
+    const u32 cnt_l = __shfl_sync(FULL_MASK, act ? q.cnt[u] : 0u, last);
+    const u32 u_l = __shfl_sync(FULL_MASK, u, last);
+    const bool memo = n >= 3 && lane + 2 == n && crow == 0xFFFFFFFFu && cm_all != 0 && bm_ok && cm_l != 0 &&
+                      crow_l != 0xFFFFFFFFu && cnt_l <= PSM_MEMO_CAP;
+    if (memo) cm = cm_all;
+    const u32 memo_any = __ballot_sync(FULL_MASK, memo);
     u32 inval = 0;
     for (u32 x = 0; x < n; ++x) {
         const u32 bal = __ballot_sync(FULL_MASK, act && cm != 0 && cdep >= x);
@@ -924,7 +936,11 @@ __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
         q.crow[lane] = crow;
         q.cinval[lane] = inval;
     }
-    if (lane == 0) q.bm_depths = bm_depths;
+    if (lane == 0) {
+        q.bm_depths = bm_depths;
+        q.memo_ok = memo_any ? 1u : 0u;
+    }
+    if (memo) q.memo_tab = table_base(q, u_l, u);
     // memory cost: candidates of every vertex, both tables of every edge
     // (the query's; a unit keeps the value it was given)
     u64 mem = 0;

@@ -25,6 +25,7 @@
 #define PSM_TRACE_STEPS 256  // preparation steps recorded when tracing (+1 start stamp)
 #define HYBRID_REQUEST 0xFFFFFFFFu  // QState.step_cursor on entry: use the hybrid grid driver
 #define PSM_CACHE_BM_BITS 32768u    // candidate positions covered by an enumerator cache bitmap
+#define PSM_MEMO_CAP 8192u          // last-depth candidates covered by the per-warp weight memo
 
 typedef uint32_t u32;
 typedef uint64_t u64;
@@ -154,6 +155,14 @@ struct QState {
     u32 crow[PSM_MAXQ];
     u32 cinval[PSM_MAXQ];
     u32 bm_depths;                        // depths with |C(u_d)| <= PSM_CACHE_BM_BITS
+    // Last-two-depth weight memo (d = n-2, l = n-1): when C(u_d) depends only
+    // on depths <= d-2 (its cache S_d) and depth l intersects its cache S_l
+    // with the row of the depth-d vertex, the completions below a depth-(d-1)
+    // node are sum over x in S_l of w(x) = |T[u_l -> u_d][x] ∩ S_d| (less
+    // exact corrections for used vertices); w is memoised per warp while S_d
+    // stays valid. memo_ok enables it; memo_tab = row base of T[u_l -> u_d].
+    u32 memo_ok;
+    u32 memo_tab;
     u32 root_cnt;
     // results
     u64 count;
