@@ -53,6 +53,17 @@ REF_THREADS_NOTE = ("-threadnums 1: multi-threaded reference runs of capped quer
                     "until the time limit, so one thread is the reference's fastest exact configuration")
 
 
+def enum_traffic():
+    """Mean DRAM bytes per enum_kernel launch of this workload, from the ncu
+    capture summarised in profiles/ (None if absent)."""
+    p = ROOT / "profiles" / "enum_kernel_traffic_plain_rmat_s20.md"
+    if p.exists():
+        m = re.search(r"traffic_bytes_per_launch: (\d+)", p.read_text())
+        if m:
+            return int(m.group(1))
+    return None
+
+
 def peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -314,7 +325,10 @@ def ours_arm(args, world, rank, local):
             # per plain-path query: prep, enum-init, enum, gather kernels + 2 memsets
             "gpu_launches": 4 * nq * args.steps,
             "roofline": {"bound": "hbm", "kernel": "enum_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None},
+                         "frac": achieved / hbm, "peak_kind": peak_kind,
+                         # ncu DRAM bytes per launch (profiles/) against the
+                         # algorithmic bytes per launch of this run
+                         "traffic": enum_traffic(), "alg_bytes_per_launch": alg / (nq * args.steps)},
             "clocks": clk}
     # Batched path on the same queries: one preparation launch + one
     # enumeration launch for the whole step (device time, CUDA events).
