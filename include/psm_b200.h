@@ -92,6 +92,20 @@ const char* psm_version(void);
 int psm_graph_from_csr(const uint32_t* offsets, const uint32_t* neighbors, const uint32_t* labels,
                        uint32_t num_vertices, psm_graph** out);
 int psm_graph_load(const char* path, psm_graph** out); /* reference text format */
+/* The reference's binary graph format (Graph::loadGraphFromFileCompressed,
+ * graph/graph.cpp:221-310): degree file (int32 4, uint32 |V|, uint32 |E|,
+ * uint32 degree[|V|]), adjacency file (uint32 neighbours row by row), label
+ * file (uint32 label[|V|]). */
+int psm_graph_load_binary(const char* degree_path, const char* adjacency_path, const char* label_path,
+                          psm_graph** out);
+/* Writes an undirected CSR in that format (Graph::storeComparessedGraph,
+ * graph/graph.cpp:355-403). Host only. */
+int psm_graph_store_binary(const uint32_t* offsets, const uint32_t* neighbors, const uint32_t* labels,
+                           uint32_t num_vertices, const char* degree_path, const char* adjacency_path,
+                           const char* label_path);
+/* Text graph -> <prefix>_deg.bin, <prefix>_adj.bin, <prefix>_label.bin
+ * (replaces matching/GraphConverter.cpp). Host only. */
+int psm_graph_convert(const char* text_path, const char* out_prefix);
 int psm_graph_info(const psm_graph* g, uint32_t* num_vertices, uint64_t* num_edges, uint32_t* num_labels,
                    uint32_t* max_degree, uint32_t* max_label_frequency);
 void psm_graph_free(psm_graph* g);

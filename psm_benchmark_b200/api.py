@@ -65,6 +65,14 @@ class DataGraph:
         N.check(N.lib().psm_graph_load(str(path).encode(), C.byref(h)))
         return cls(h)
 
+    @classmethod
+    def load_binary(cls, prefix) -> "DataGraph":
+        """Reference binary format: <prefix>_deg.bin, _adj.bin, _label.bin."""
+        h = C.c_void_p()
+        N.check(N.lib().psm_graph_load_binary(f"{prefix}_deg.bin".encode(), f"{prefix}_adj.bin".encode(),
+                                              f"{prefix}_label.bin".encode(), C.byref(h)))
+        return cls(h)
+
     def info(self):
         V, L, md, mf = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
         E = C.c_uint64()
@@ -369,3 +377,20 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------- graph file formats --
+
+def store_binary(g: Graph, prefix) -> None:
+    """Writes g in the reference's binary format (host only)."""
+    off = np.ascontiguousarray(g.off, np.uint32)
+    nbr = np.ascontiguousarray(g.nbr, np.uint32)
+    lab = np.ascontiguousarray(g.labels, np.uint32)
+    N.check(N.lib().psm_graph_store_binary(_u32p(off), _u32p(nbr), _u32p(lab), g.num_vertices,
+                                           f"{prefix}_deg.bin".encode(), f"{prefix}_adj.bin".encode(),
+                                           f"{prefix}_label.bin".encode()))
+
+
+def convert_text(text_path, prefix) -> None:
+    """Text graph -> reference binary files (the reference's GraphConverter)."""
+    N.check(N.lib().psm_graph_convert(str(text_path).encode(), str(prefix).encode()))

@@ -20,6 +20,11 @@
 int psm_graph_build(const uint32_t* off, const uint32_t* nbr, const uint32_t* labels, uint32_t V, psm_graph** out,
                     std::string* err);
 int psm_graph_parse(const char* path, psm_graph** out, std::string* err);
+int psm_graph_parse_binary(const char* deg_path, const char* adj_path, const char* label_path, psm_graph** out,
+                           std::string* err);
+int psm_text_to_binary(const char* text_path, const char* out_prefix, std::string* err);
+int psm_csr_write_binary(const u32* off, const u32* nbr, const u32* labels, u32 V, const char* deg_path,
+                         const char* adj_path, const char* label_path, std::string* err);
 void psm_graph_destroy(psm_graph* g);
 
 namespace {
@@ -391,6 +396,33 @@ int psm_graph_load(const char* path, psm_graph** out) {
     if (!path || !out) return fail(PSM_ERR_ARG, "null argument");
     std::string err;
     int rc = psm_graph_parse(path, out, &err);
+    return rc ? fail(rc, err) : PSM_OK;
+}
+
+int psm_graph_load_binary(const char* degree_path, const char* adjacency_path, const char* label_path,
+                          psm_graph** out) {
+    if (!degree_path || !adjacency_path || !label_path || !out) return fail(PSM_ERR_ARG, "null argument");
+    std::string err;
+    int rc = psm_graph_parse_binary(degree_path, adjacency_path, label_path, out, &err);
+    return rc ? fail(rc, err) : PSM_OK;
+}
+
+int psm_graph_store_binary(const uint32_t* offsets, const uint32_t* neighbors, const uint32_t* labels,
+                           uint32_t num_vertices, const char* degree_path, const char* adjacency_path,
+                           const char* label_path) {
+    if (!offsets || !labels || (!neighbors && offsets[num_vertices]) || !degree_path || !adjacency_path ||
+        !label_path)
+        return fail(PSM_ERR_ARG, "null argument");
+    std::string err;
+    int rc = psm_csr_write_binary(offsets, neighbors, labels, num_vertices, degree_path, adjacency_path, label_path,
+                                  &err);
+    return rc ? fail(rc, err) : PSM_OK;
+}
+
+int psm_graph_convert(const char* text_path, const char* out_prefix) {
+    if (!text_path || !out_prefix) return fail(PSM_ERR_ARG, "null argument");
+    std::string err;
+    int rc = psm_text_to_binary(text_path, out_prefix, &err);
     return rc ? fail(rc, err) : PSM_OK;
 }
 

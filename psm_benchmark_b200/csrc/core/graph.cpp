@@ -148,7 +148,13 @@ int psm_graph_build(const uint32_t* off, const uint32_t* nbr, const uint32_t* la
 // Reference text format (graph/graph.cpp:92-172): "t V E", "v id label deg"
 // lines, then "e u v" lines. Edges are stored in both directions; rows are
 // sorted; duplicate edges are kept as the reference keeps them.
-int psm_graph_parse(const char* path, psm_graph** out, std::string* err) {
+// Host CSR of a graph file (original ids; rows sorted).
+struct HostCsr {
+    u32 V = 0;
+    std::vector<u32> off, nbr, labels;
+};
+
+int parse_text(const char* path, HostCsr* g, std::string* err) {
     FILE* f = fopen(path, "rb");
     if (!f) {
         *err = std::string("cannot open ") + path;
@@ -218,7 +224,127 @@ int psm_graph_parse(const char* path, psm_graph** out, std::string* err) {
         nbr[cur[dst[i]]++] = src[i];
     }
     for (u32 v = 0; v < V; ++v) std::sort(nbr.begin() + off[v], nbr.begin() + off[v + 1]);
-    return psm_graph_build(off.data(), nbr.data(), labels.data(), V, out, err);
+    g->V = V;
+    g->off = std::move(off);
+    g->nbr = std::move(nbr);
+    g->labels = std::move(labels);
+    return PSM_OK;
+}
+
+int psm_graph_parse(const char* path, psm_graph** out, std::string* err) {
+    HostCsr h;
+    int rc = parse_text(path, &h, err);
+    if (rc) return rc;
+    return psm_graph_build(h.off.data(), h.nbr.data(), h.labels.data(), h.V, out, err);
+}
+
+// The reference's binary graph format (Graph::loadGraphFromFileCompressed /
+// storeComparessedGraph, graph/graph.cpp:221-403; written by its
+// GraphConverter, matching/GraphConverter.cpp): a degree file (int32 size of
+// int = 4, uint32 |V|, uint32 |E| (undirected), uint32 degree[|V|]), an
+// adjacency file (uint32 neighbours, row after row, 2|E| in all) and a label
+// file (uint32 label[|V|]). Rows are sorted on load, as the reference does.
+int read_binary(const char* deg_path, const char* adj_path, const char* label_path, HostCsr* g, std::string* err) {
+    auto open = [&](const char* p) -> FILE* {
+        FILE* f = fopen(p, "rb");
+        if (!f) *err = std::string("cannot open ") + p;
+        return f;
+    };
+    FILE* fd = open(deg_path);
+    if (!fd) return PSM_ERR_IO;
+    int32_t int_size = 0;
+    u32 V = 0, E = 0;
+    bool ok = fread(&int_size, 4, 1, fd) == 1 && fread(&V, 4, 1, fd) == 1 && fread(&E, 4, 1, fd) == 1;
+    std::vector<u32> deg(V);
+    ok = ok && int_size == 4 && (V == 0 || fread(deg.data(), 4, V, fd) == V);
+    fclose(fd);
+    if (!ok) {
+        *err = std::string("malformed degree file ") + deg_path;
+        return PSM_ERR_IO;
+    }
+    std::vector<u32> off(V + 1, 0);
+    for (u32 v = 0; v < V; ++v) off[v + 1] = off[v] + deg[v];
+    if ((u64)off[V] != 2ull * E) {
+        *err = "degree sum differs from 2|E|";
+        return PSM_ERR_IO;
+    }
+    std::vector<u32> nbr(off[V]);
+    FILE* fa = open(adj_path);
+    if (!fa) return PSM_ERR_IO;
+    ok = nbr.empty() || fread(nbr.data(), 4, nbr.size(), fa) == nbr.size();
+    fclose(fa);
+    if (!ok) {
+        *err = std::string("short adjacency file ") + adj_path;
+        return PSM_ERR_IO;
+    }
+    std::vector<u32> labels(V);
+    FILE* fl = open(label_path);
+    if (!fl) return PSM_ERR_IO;
+    ok = V == 0 || fread(labels.data(), 4, V, fl) == V;
+    fclose(fl);
+    if (!ok) {
+        *err = std::string("short label file ") + label_path;
+        return PSM_ERR_IO;
+    }
+    for (u32 v = 0; v < V; ++v) std::sort(nbr.begin() + off[v], nbr.begin() + off[v + 1]);
+    g->V = V;
+    g->off = std::move(off);
+    g->nbr = std::move(nbr);
+    g->labels = std::move(labels);
+    return PSM_OK;
+}
+
+int write_binary(const u32* off, const u32* nbr, const u32* labels, u32 V, const char* deg_path, const char* adj_path,
+                 const char* label_path, std::string* err) {
+    if ((off[V] & 1u) != 0) {
+        *err = "odd number of adjacency entries (an undirected CSR stores every edge twice)";
+        return PSM_ERR_ARG;
+    }
+    const int32_t int_size = 4;
+    const u32 E = off[V] / 2;
+    std::vector<u32> deg(V);
+    for (u32 v = 0; v < V; ++v) deg[v] = off[v + 1] - off[v];
+    auto put = [&](const char* p, const void* a, size_t n, const void* h, size_t hn) -> bool {
+        FILE* f = fopen(p, "wb");
+        if (!f) {
+            *err = std::string("cannot write ") + p;
+            return false;
+        }
+        bool ok = (hn == 0 || fwrite(h, 1, hn, f) == hn) && (n == 0 || fwrite(a, 4, n, f) == n);
+        ok = (fclose(f) == 0) && ok;
+        if (!ok) *err = std::string("write failed: ") + p;
+        return ok;
+    };
+    char head[12];
+    memcpy(head, &int_size, 4);
+    memcpy(head + 4, &V, 4);
+    memcpy(head + 8, &E, 4);
+    if (!put(deg_path, deg.data(), V, head, 12) || !put(adj_path, nbr, off[V], nullptr, 0) ||
+        !put(label_path, labels, V, nullptr, 0))
+        return PSM_ERR_IO;
+    return PSM_OK;
+}
+
+int psm_graph_parse_binary(const char* deg_path, const char* adj_path, const char* label_path, psm_graph** out,
+                           std::string* err) {
+    HostCsr h;
+    int rc = read_binary(deg_path, adj_path, label_path, &h, err);
+    if (rc) return rc;
+    return psm_graph_build(h.off.data(), h.nbr.data(), h.labels.data(), h.V, out, err);
+}
+
+int psm_text_to_binary(const char* text_path, const char* out_prefix, std::string* err) {
+    HostCsr h;
+    int rc = parse_text(text_path, &h, err);
+    if (rc) return rc;
+    const std::string pre(out_prefix);
+    return write_binary(h.off.data(), h.nbr.data(), h.labels.data(), h.V, (pre + "_deg.bin").c_str(),
+                        (pre + "_adj.bin").c_str(), (pre + "_label.bin").c_str(), err);
+}
+
+int psm_csr_write_binary(const u32* off, const u32* nbr, const u32* labels, u32 V, const char* deg_path,
+                         const char* adj_path, const char* label_path, std::string* err) {
+    return write_binary(off, nbr, labels, V, deg_path, adj_path, label_path, err);
 }
 
 void psm_graph_destroy(psm_graph* g) { free_graph(g); }

@@ -28,6 +28,7 @@ EXPORTS = [
     "psm_match_join", "psm_query_decompose", "psm_hash_join",
     "psm_server_create", "psm_server_submit", "psm_server_poll", "psm_server_pending", "psm_server_estimate",
     "psm_server_clock_ns", "psm_server_destroy",
+    "psm_graph_load_binary", "psm_graph_store_binary", "psm_graph_convert",
 ]
 MAX_UNITS = 32
 
@@ -91,6 +92,9 @@ def lib():
         "psm_version": ([], C.c_char_p),
         "psm_graph_from_csr": ([u32p, u32p, u32p, C.c_uint32, C.POINTER(vp)], C.c_int),
         "psm_graph_load": ([C.c_char_p, C.POINTER(vp)], C.c_int),
+        "psm_graph_load_binary": ([C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(vp)], C.c_int),
+        "psm_graph_store_binary": ([u32p, u32p, u32p, C.c_uint32, C.c_char_p, C.c_char_p, C.c_char_p], C.c_int),
+        "psm_graph_convert": ([C.c_char_p, C.c_char_p], C.c_int),
         "psm_graph_info": ([vp, u32p, C.POINTER(C.c_uint64), u32p, u32p, u32p], C.c_int),
         "psm_graph_free": ([vp], None),
         "psm_context_create": ([C.c_int, C.c_uint64, C.POINTER(vp)], C.c_int),
