@@ -469,6 +469,15 @@ int psm_context_create(int device, uint64_t arena_bytes, psm_context** out) {
         psm_context_free(c);
         return fail(PSM_ERR_CUDA, "occupancy query failed");
     }
+    // Plain-path preparation grid: one block of 512 per SM. Its steps are
+    // small, so the grid barrier's cost sets their time: measured on B200,
+    // 148 blocks prepare the benchmark queries 13 % faster than 296 (and 74 or
+    // a 16-block cluster are slower). PSM_PREP_BLOCKS overrides the size.
+    c->prep_grid_blocks = std::min(c->prep_grid_blocks, prop.multiProcessorCount);
+    if (const char* pb = getenv("PSM_PREP_BLOCKS")) {
+        const int want = atoi(pb);
+        if (want > 0) c->prep_grid_blocks = std::min(std::max(c->prep_grid_blocks, want), want);
+    }
     c->prep_block_blocks = prop.multiProcessorCount * 4;
     // Batched preparation team: clusters of 8 blocks per query (default), or
     // one block per query (PSM_BATCH_TEAM=block).
