@@ -473,10 +473,11 @@ int psm_context_create(int device, uint64_t arena_bytes, psm_context** out) {
     // small, so the grid barrier's cost sets their time: measured on B200,
     // 148 blocks prepare the benchmark queries 13 % faster than 296 (and 74 or
     // a 16-block cluster are slower). PSM_PREP_BLOCKS overrides the size.
-    c->prep_grid_blocks = std::min(c->prep_grid_blocks, prop.multiProcessorCount);
+    const int coresident = c->prep_grid_blocks;  // cooperative launch limit
+    c->prep_grid_blocks = std::min(coresident, prop.multiProcessorCount);
     if (const char* pb = getenv("PSM_PREP_BLOCKS")) {
         const int want = atoi(pb);
-        if (want > 0) c->prep_grid_blocks = std::min(std::max(c->prep_grid_blocks, want), want);
+        if (want > 0) c->prep_grid_blocks = std::min(coresident, want);
     }
     c->prep_block_blocks = prop.multiProcessorCount * 4;
     // Batched preparation team: clusters of 8 blocks per query (default), or
