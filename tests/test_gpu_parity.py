@@ -142,13 +142,17 @@ def test_algorithmic_bytes_match_oracle(engine):
                     assert got.alg_bytes == int(ref.depth_bytes.sum()), (f, o)
     finally:
         plain_engine.close()
+    # every plain_small query under both methods: these include orders whose
+    # last two depths are counted through the weight memo
     syn = gd.synthetic_graph("plain_small")
     og = OracleGraph(syn)
     dg = api.DataGraph.from_graph(syn)
     case = dict(gd.synthetic_cases())["plain_small"]
-    for entry in case["queries"][:12]:
+    for entry in case["queries"]:
         q = gd.query_from_rec(entry["query"])
-        ref = og.run(q, "GQL", "GQL", want_tables=False)
-        got = api.match(engine, dg, q, "GQL_GQL_GQL")
-        assert got.count == ref.count
-        assert got.alg_bytes == int(ref.depth_bytes.sum())
+        for f, m in (("GQL", "GQL_GQL_GQL"), ("CFL", "CFL_CFL_EXPLORE")):
+            ref = og.run(q, f, f, cap=entry["cap"], want_tables=False)
+            got = api.match(engine, dg, q, m, cap=entry["cap"])
+            assert got.count == ref.count
+            if not entry["cap"] or ref.count < entry["cap"]:
+                assert got.alg_bytes == int(ref.depth_bytes.sum()), (m, q.num_vertices)
