@@ -583,8 +583,8 @@ def main():
     ap.add_argument("--no-batched", dest="batched", action="store_false")
     ap.add_argument("--only", default="", help="comma-separated query indices (profiling runs)")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "join", "serve"])
-    ap.add_argument("--lanes", type=int, default=1, help="serving lanes")
-    ap.add_argument("--max-batch", type=int, default=512, help="serving batch limit")
+    ap.add_argument("--lanes", type=int, default=4, help="serving lanes")
+    ap.add_argument("--max-batch", type=int, default=64, help="serving batch limit")
     ap.add_argument("--serve-budget-gb", type=int, default=120, help="serving device-memory budget")
     args = ap.parse_args()
     world, rank, local = dist_setup()
