@@ -343,6 +343,7 @@ def ours_arm(args, world, rank, local):
     if bres is not None:
         if [r.count for r in bres] != counts:
             raise SystemExit("batched counts differ from the plain path")
+        bt = max_over_ranks([bt], dist, device=f"cuda:{local}")[0]
         bval = world * nq * args.steps / (bt / 1e3)
         line["batched"] = {"value": bval, "unit": "queries/s", "ms_per_step": bt / args.steps,
                            "speedup_vs_plain": bval / value, "launches_per_step": 4}
