@@ -12,8 +12,9 @@ sequence. Synthetic data generated from fixed seeds (no dataset download).
 One step = the 200 queries through the plain path. `value` is queries/s
 from the device time of the launches (CUDA events on the library's stream,
 graph resident in HBM); `e2e` is the same through the C ABI call psm_match
-with host query buffers, host->device descriptor copies and device->host
-result reads inside the wall-clock timed region. The data graph (72 MB) fits
+with host query buffers, host->device descriptor copies (through the
+context's pinned staging buffer) and device->host result reads inside the
+wall-clock timed region. The data graph (72 MB) fits
 in L2, so L2 is flushed (256 MiB write) before every timed step. With N GPUs
 each rank runs the whole workload on its own replica of the graph (replicas
 only, weak scaling); times are the max over ranks.

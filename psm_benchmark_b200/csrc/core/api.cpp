@@ -85,7 +85,8 @@ struct psm_context {
     int batch_clusters = 0;  // clusters of that launch
     int enum_blocks = 0;
     cudaEvent_t ev[4]{};
-    std::vector<char> host_stage;  // QDesc / QState staging
+    char* pinned = nullptr;  // pinned host staging of descriptors, states and results
+    size_t pinned_bytes = 0;
     bool run_live = false;
 };
 
@@ -208,6 +209,23 @@ void fill_result(const DevResult& r, float prep_ms, float enum_ms, u64 donations
     out->enum_ms = enum_ms;
 }
 
+// Pinned host staging of at least `bytes` (the context's stream is idle
+// between calls, so the buffer can be replaced here).
+char* staging(psm_context* ctx, size_t bytes) {
+    if (bytes <= ctx->pinned_bytes) return ctx->pinned;
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    size_t want = std::max<size_t>(bytes, 1 << 20);
+    if (cudaHostAlloc((void**)&ctx->pinned, want, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->pinned = nullptr;
+        return nullptr;
+    }
+    ctx->pinned_bytes = want;
+    return ctx->pinned;
+}
+
 // Runs nq queries. grid_team: prepare the (single) query with the whole grid
 // (plain path); otherwise one block per query (batched path).
 int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, u32 nq, const psm_options& opt,
@@ -249,11 +267,27 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     da.base = (u32*)(ctx->arena + start);
     da.top = 0;
     da.cap = (b.cap - start) / sizeof(u32);
-    // uploads: descriptors (used prefix only), states, allocator, barrier
-    for (u32 i = 0; i < nq; ++i)
-        CK(cudaMemcpyAsync(lay.d_desc + i, &descs[i], psm_qdesc_bytes(descs[i]), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(lay.d_q, hq.data(), sizeof(QState) * nq, cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaMemcpyAsync(ctx->d_devarena, &da, sizeof(da), cudaMemcpyHostToDevice, ctx->st));
+    // uploads from pinned staging: descriptors (used prefix only), states,
+    // allocator; the results come back through the same buffer
+    size_t desc_bytes = 0;
+    for (u32 i = 0; i < nq; ++i) desc_bytes += align_up(psm_qdesc_bytes(descs[i]), 16);
+    const size_t off_q = align_up(desc_bytes), off_a = off_q + align_up(sizeof(QState) * nq),
+                 off_r = off_a + align_up(sizeof(DevArena));
+    char* pin = staging(ctx, off_r + sizeof(DevResult) * nq);
+    if (!pin) return fail(PSM_ERR_OOM, "pinned host staging");
+    {
+        size_t o = 0;
+        for (u32 i = 0; i < nq; ++i) {
+            const size_t b = psm_qdesc_bytes(descs[i]);
+            memcpy(pin + o, &descs[i], b);
+            CK(cudaMemcpyAsync(lay.d_desc + i, pin + o, b, cudaMemcpyHostToDevice, ctx->st));
+            o += align_up(b, 16);
+        }
+    }
+    memcpy(pin + off_q, hq.data(), sizeof(QState) * nq);
+    memcpy(pin + off_a, &da, sizeof(da));
+    CK(cudaMemcpyAsync(lay.d_q, pin + off_q, sizeof(QState) * nq, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->d_devarena, pin + off_a, sizeof(da), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemsetAsync(ctx->d_barrier, 0, 64, ctx->st));
     CK(cudaMemsetAsync(ctx->d_ticket, 0, sizeof(u32), ctx->st));
     const u64 budget = budget_ns(opt);
@@ -289,12 +323,13 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
         poll(poll_arg);
     }
     std::vector<DevResult> res(nq);
-    CK(cudaMemcpyAsync(res.data(), lay.d_res, sizeof(DevResult) * nq, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaMemcpyAsync(pin + off_r, lay.d_res, sizeof(DevResult) * nq, cudaMemcpyDeviceToHost, ctx->st));
     EnumStats es{};
     if (prep_only)
         CK(cudaStreamSynchronize(ctx->st));
     else
-        CK(psm_enum_read_ctl(ctx->d_enum_scratch, &es, ctx->st));
+        CK(psm_enum_read_ctl(ctx->d_enum_scratch, &es, ctx->st));  // synchronises the stream
+    memcpy(res.data(), pin + off_r, sizeof(DevResult) * nq);
     const u32 enum_err = es.error;
     float prep_ms = 0, enum_ms = 0;
     CK(cudaEventElapsedTime(&prep_ms, ctx->ev[0], ctx->ev[1]));
@@ -521,6 +556,7 @@ void psm_context_free(psm_context* c) {
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     if (c->arena) cudaFree(c->arena);
+    if (c->pinned) cudaFreeHost(c->pinned);
     if (c->d_enum_cache) cudaFree(c->d_enum_cache);
     if (c->st) cudaStreamDestroy(c->st);
     delete c;
