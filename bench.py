@@ -254,7 +254,9 @@ def ours_arm(args, world, rank, local):
     if world > 1:
         import torch.distributed as dist
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # collectives here are seconds apart: a short timeout ends a run whose
+        # rank failed instead of leaving the others waiting
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     from psm_benchmark_b200 import api
     w = make_workload(args)
     eng = api.Engine(device=local, arena_bytes=args.arena_gb << 30)
