@@ -55,6 +55,44 @@ __device__ __forceinline__ void label_run(const DevGraph& g, u32 v, u32 l, u32& 
     e = lower_bound_u32(g.nbr, s, hi, g.lab_off[l + 1]);
 }
 
+// lower_bound_u32 computed by the 8 lanes of an aligned lane group together:
+// each round probes 8 evenly spaced positions of the range (a 9-way split),
+// so a row of 1,000 entries takes 4 dependent loads instead of 10. Called
+// by the whole warp; lo, hi and key are uniform within each group, and a
+// group with lo == hi loads nothing.
+__device__ __forceinline__ u32 group_lower_bound(const u32* __restrict__ a, u32 lo, u32 hi, u32 key) {
+    const u32 lg = lane_id() & 7u, sh = lane_id() & 24u;
+    while (__any_sync(FULL_MASK, hi - lo > 8u)) {
+        const u32 n = hi - lo;
+        // probes lo + floor(n (j + 1) / 9), j = 0..7: distinct, inside (lo, hi)
+        bool lt = false;
+        if (n > 8u) lt = __ldg(a + lo + (u32)((u64)n * (lg + 1u) / 9u)) < key;
+        const u32 c = __popc((__ballot_sync(FULL_MASK, lt) >> sh) & 0xffu);  // probes below key: a prefix
+        if (n > 8u) {
+            const u32 nlo = c ? lo + (u32)((u64)n * c / 9u) + 1u : lo;
+            const u32 nhi = c < 8u ? lo + (u32)((u64)n * (c + 1u) / 9u) : hi;
+            lo = nlo;
+            hi = nhi;
+        }
+    }
+    const bool lt = lg < hi - lo && __ldg(a + lo + lg) < key;
+    return lo + __popc((__ballot_sync(FULL_MASK, lt) >> sh) & 0xffu);
+}
+
+// label_run for the 8-lane group of this lane (v and l group-uniform; a
+// group with !valid gets an empty run). Called by the whole warp.
+__device__ __forceinline__ void group_label_run(const DevGraph& g, bool valid, u32 v, u32 l, u32& s, u32& e) {
+    u32 lo = 0, hi = 0, k1 = 0, k2 = 0;
+    if (valid && l < g.L) {
+        lo = g.off[v];
+        hi = g.off[v + 1];
+        k1 = g.lab_off[l];
+        k2 = g.lab_off[l + 1];
+    }
+    s = group_lower_bound(g.nbr, lo, hi, k1);
+    e = group_lower_bound(g.nbr, s, hi, k2);
+}
+
 __device__ __forceinline__ bool test_bit(const u32* bm, u32 pos) { return (bm[pos >> 5] >> (pos & 31)) & 1u; }
 
 __device__ __forceinline__ u32 warp_sum(u32 x) {

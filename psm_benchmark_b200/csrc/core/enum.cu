@@ -100,6 +100,15 @@ constexpr u32 WARP_CACHE_WORDS = PSM_MAXQ * SLOT_WORDS + PSM_MEMO_CAP;  // slots
 constexpr u32 NO_ROW = 0xFFFFFFFFu;
 constexpr u32 LONG_ROW = 24;     // per-lane binary-search walks longer than this go to the warp
 constexpr u32 LONG_BM_ROW = 96;  // per-lane bitmap walks longer than this go to the warp
+// With only `act` lanes holding a candidate, a lane's walk costs the warp its
+// whole length while the cooperative walk costs about 1/32 of it plus a fixed
+// setup: walks longer than these multiples of `act` go to the warp too.
+#ifndef PSM_DEFER_BM_K
+#define PSM_DEFER_BM_K 8
+#endif
+#ifndef PSM_DEFER_ROW_K
+#define PSM_DEFER_ROW_K 2
+#endif
 
 // Invariants of the cache state: cvalid bit d => S of depth d is the
 // intersection for the current prefix; cbits bit d => the bitmap of depth d
@@ -532,9 +541,11 @@ __device__ __forceinline__ u32 cached_exclusions(const QState& q, u32 dl, u32 v,
 }
 
 __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 v, const WarpStack* ws, u64& bytes,
-                               u64& calls, bool* defer) {
+                               u64& calls, bool* defer, u32 act) {
     const u32 nb = q.nbn[dl];
     const u32 dp = dl - 1;
+    const u32 long_bm = min(LONG_BM_ROW, PSM_DEFER_BM_K * act);
+    const u32 long_row = min(LONG_ROW, max(2u, PSM_DEFER_ROW_K * act));
     if (cached) {
         const u32 s = ws->clen[dl];
         const u32 k = q.crow[dl];
@@ -550,7 +561,7 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
         u64 c = 0;
         if (walk_r_with_bitmap(ws, dl, r, s)) {
             calls += r;
-            if (r > LONG_BM_ROW) {
+            if (r > long_bm) {
                 *defer = true;
                 return 0;
             }
@@ -558,7 +569,7 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
             for (u32 e = lo; e < hi; ++e) c += bm_test(bm, __ldg(q.adj + e));
         } else {
             calls += min(s, r);
-            if (min(s, r) > LONG_ROW) {
+            if (min(s, r) > long_row) {
                 *defer = true;
                 return 0;
             }
@@ -583,7 +594,7 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
     bytes += by;
     calls += blen;
     if (blen == 0) return 0;
-    if (nb > 1 && blen > LONG_ROW) {
+    if (nb > 1 && blen > long_row) {
         *defer = true;
         return 0;
     }
@@ -1022,7 +1033,8 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
                 const u32 p = valid ? (d == 0 ? idx : drv_elem(q, ws, d, idx)) : 0u;
                 const bool ok = d == 0 ? valid : chunk_accept(q, d, p, valid, ws, list_d);
                 const u32 v = ok ? list_d[p] : 0u;
-                if (ok) c = lane_last_count(q, d + 1, cached, p, v, ws, bytes_l, calls_l, &defer);
+                const u32 act = __popc(__ballot_sync(FULL_MASK, ok));
+                if (ok) c = lane_last_count(q, d + 1, cached, p, v, ws, bytes_l, calls_l, &defer, act);
                 count += warp_sum64(c);
                 // long intersections deferred by their lanes: whole warp each
                 u32 dm = __ballot_sync(FULL_MASK, defer);

@@ -190,6 +190,29 @@ __device__ bool nlf_ok(const DevGraph& g, const QDesc* d, u32 t, u32 v) {
     return true;
 }
 
+// nlf_ok for the 8-lane group of this lane (t uniform in the warp, v and
+// valid uniform in the group); the label runs come from group_lower_bound.
+// Called by the whole warp.
+__device__ bool group_nlf_ok(const DevGraph& g, const QDesc* d, u32 t, bool valid, u32 v) {
+    u32 lo = 0, hi = 0;
+    if (valid) {
+        lo = g.off[v];
+        hi = g.off[v + 1];
+    }
+    bool ok = valid && hi - lo >= d->item_deg[t];
+    for (u32 k = d->nlf_off[t]; k < d->nlf_off[t + 1]; ++k) {
+        if (!__any_sync(FULL_MASK, ok)) break;
+        const u32 l = d->nlf_lab[k], need = d->nlf_cnt[k];
+        if (l >= g.L) ok = false;
+        const u32 s = group_lower_bound(g.nbr, ok ? lo : 0u, ok ? hi : 0u, ok ? g.lab_off[l] : 0u);
+        if (ok && hi - s < need) ok = false;
+        const u32 e = group_lower_bound(g.nbr, ok ? s : 0u, ok ? hi : 0u, ok ? g.lab_off[l + 1] : 0u);
+        if (ok && e - s < need) ok = false;
+        if (ok) lo = e;
+    }
+    return ok;
+}
+
 __device__ __forceinline__ u32 bucket_size(const DevGraph& g, u32 l) {
     return l < g.L ? g.lab_off[l + 1] - g.lab_off[l] : 0u;
 }
@@ -340,11 +363,13 @@ __device__ bool mark_neighbours(Team& t, const DevGraph& g, QState& q, u32 p, u3
     const u32 N = q.cnt[p];
     for (u32 i0 = t.warp() * 4u; i0 < N; i0 += t.nwarps() * 4u) {
         u32 i = i0 + grp;
-        u32 s = 0, e = 0;
+        u32 c = 0, s, e;
+        bool live = false;
         if (i < N) {
-            u32 c = q.list[p][i];
-            if (test_bit(q.bm[p], c - base_p)) label_run(g, c, lu, s, e);
+            c = q.list[p][i];
+            live = test_bit(q.bm[p], c - base_p);
         }
+        group_label_run(g, live, c, lu, s, e);
         u32 len = e - s;
         u32 mx = warp_max(len);
         for (u32 j = 0; j < mx; j += 8) {
@@ -455,10 +480,24 @@ __device__ bool step_generate(Team& t, const DevGraph& g, QState& q, u32 u, u32 
     const u32 lane = lane_id();
     const u32 base = bucket_base(g, lu), bsz = bucket_size(g, lu);
     const u32 per_blk = scan_block_words(W, t.nblocks());
+    const u32 grp = lane >> 3, lg = lane & 7u;
     for (u32 w = t.warp(); w < W; w += t.nwarps()) {
-        u32 pos = 32u * w + lane;
-        bool ok = pos < bsz && ((q.acc[w] >> lane) & 1u) && nlf_ok(g, d, u, base + pos);
-        u32 word = __ballot_sync(FULL_MASK, ok);
+        u32 bits = q.acc[w];
+        if (bsz - 32u * w < 32u) bits &= (1u << (bsz - 32u * w)) - 1u;  // W words cover bsz bits
+        u32 word = 0;
+        if (__popc(bits) > 8u) {  // dense word: a lane per bit
+            const bool ok = ((bits >> lane) & 1u) && nlf_ok(g, d, u, base + 32u * w + lane);
+            word = __ballot_sync(FULL_MASK, ok);
+        } else {
+            while (bits) {  // sparse word: a lane group per bit, 4 bits a round
+                u32 b = bits;
+                for (u32 k = 0; k < grp; ++k) b &= b - 1u;
+                const u32 bit = b ? __ffs(b) - 1u : 0u;
+                const bool ok = group_nlf_ok(g, d, u, b != 0, base + 32u * w + bit);
+                word |= __reduce_or_sync(FULL_MASK, ok && lg == 0 ? 1u << bit : 0u);
+                for (u32 k = 0; k < 4u; ++k) bits &= bits - 1u;
+            }
+        }
         if (lane == 0) {
             q.bm[u][w] = word;
             q.acc[w] = 0;
@@ -488,8 +527,8 @@ __device__ bool step_prune(Team& t, const DevGraph& g, QState& q, u32 u, u32 piv
             u32 p = __ffs(pm) - 1;
             pm &= pm - 1;
             const u32 lp = d->label[p], base_p = bucket_base(g, lp);
-            u32 s = 0, e = 0;
-            if (alive) label_run(g, v, lp, s, e);
+            u32 s, e;
+            group_label_run(g, alive, v, lp, s, e);  // alive is uniform in the group
             u32 len = e - s;
             u32 mx = warp_max(len);
             bool found = false;
@@ -564,14 +603,15 @@ __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* ar
     // count pass
     for (u32 r0 = t.warp() * 4u; r0 < R; r0 += t.nwarps() * 4u) {
         u32 r = r0 + grp;
-        u32 s = 0, e = 0, y = 0;
+        u32 s, e, y = 0, v = 0;
         if (r < R) {
             u32 ei, i;
             row_of(q, ne, r, ei, i);
             u32 x = edge_src(d, ei);
             y = d->e_dst[ei];
-            label_run(g, q.list[x][i], d->label[y], s, e);
+            v = q.list[x][i];
         }
+        group_label_run(g, r < R, v, d->label[y], s, e);
         const u32 base_y = r < R ? bucket_base(g, d->label[y]) : 0;
         u32 len = e - s, mx = warp_max(len), c = 0;
         for (u32 j = 0; j < mx; j += 8) {
@@ -606,15 +646,16 @@ __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* ar
     // fill pass
     for (u32 r0 = t.warp() * 4u; r0 < R; r0 += t.nwarps() * 4u) {
         u32 r = r0 + grp;
-        u32 s = 0, e = 0, y = 0, out = 0;
+        u32 s, e, y = 0, v = 0, out = 0;
         if (r < R) {
             u32 ei, i;
             row_of(q, ne, r, ei, i);
             u32 x = edge_src(d, ei);
             y = d->e_dst[ei];
-            label_run(g, q.list[x][i], d->label[y], s, e);
+            v = q.list[x][i];
             out = P[r];
         }
+        group_label_run(g, r < R, v, d->label[y], s, e);
         const u32 base_y = r < R ? bucket_base(g, d->label[y]) : 0;
         u32 len = e - s, mx = warp_max(len), written = 0;
         for (u32 j = 0; j < mx; j += 8) {
