@@ -372,11 +372,19 @@ __device__ bool mark_neighbours(Team& t, const DevGraph& g, QState& q, u32 p, u3
         group_label_run(g, live, c, lu, s, e);
         u32 len = e - s;
         u32 mx = warp_max(len);
-        for (u32 j = 0; j < mx; j += 8) {
-            if (j + lg < len) {
-                u32 pos = __ldg(g.nbr + s + j + lg) - base_u;
-                atomicOr(out + (pos >> 5), 1u << (pos & 31u));
+        for (u32 j = 0; j < mx; j += 32) {  // 4 loads in flight per lane
+            u32 x[4];
+#pragma unroll
+            for (u32 k = 0; k < 4; ++k) {
+                const u32 o = j + 8u * k + lg;
+                x[k] = o < len ? __ldg(g.nbr + s + o) : 0u;
             }
+#pragma unroll
+            for (u32 k = 0; k < 4; ++k)
+                if (j + 8u * k + lg < len) {
+                    const u32 pos = x[k] - base_u;
+                    atomicOr(out + (pos >> 5), 1u << (pos & 31u));
+                }
         }
     }
     return true;
@@ -532,12 +540,20 @@ __device__ bool step_prune(Team& t, const DevGraph& g, QState& q, u32 u, u32 piv
             u32 len = e - s;
             u32 mx = warp_max(len);
             bool found = false;
-            for (u32 j = 0; j < mx; j += 8) {
+            for (u32 j = 0; j < mx; j += 32) {  // 4 loads in flight per lane
+                u32 x[4];
+#pragma unroll
+                for (u32 k = 0; k < 4; ++k) {
+                    const u32 o = j + 8u * k + lg;
+                    x[k] = o < len ? __ldg(g.nbr + s + o) : 0u;
+                }
                 bool hit = false;
-                if (j + lg < len) hit = test_bit(q.bm[p], __ldg(g.nbr + s + j + lg) - base_p);
+#pragma unroll
+                for (u32 k = 0; k < 4; ++k)
+                    if (j + 8u * k + lg < len) hit |= test_bit(q.bm[p], x[k] - base_p);
                 u32 bal = __ballot_sync(FULL_MASK, hit);
                 if ((bal >> (grp * 8u)) & 0xffu) found = true;
-                if (__all_sync(FULL_MASK, found || !alive || j + 8 >= len)) break;
+                if (__all_sync(FULL_MASK, found || !alive || j + 32 >= len)) break;
             }
             if (alive && !found) alive = false;
         }
@@ -614,10 +630,18 @@ __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* ar
         group_label_run(g, r < R, v, d->label[y], s, e);
         const u32 base_y = r < R ? bucket_base(g, d->label[y]) : 0;
         u32 len = e - s, mx = warp_max(len), c = 0;
-        for (u32 j = 0; j < mx; j += 8) {
-            bool hit = j + lg < len && test_bit(q.bm[y], __ldg(g.nbr + s + j + lg) - base_y);
-            u32 bal = __ballot_sync(FULL_MASK, hit);
-            c += __popc((bal >> (grp * 8u)) & 0xffu);
+        for (u32 j = 0; j < mx; j += 32) {  // 4 loads in flight per lane
+            u32 x[4];
+#pragma unroll
+            for (u32 k = 0; k < 4; ++k) {
+                const u32 o = j + 8u * k + lg;
+                x[k] = o < len ? __ldg(g.nbr + s + o) : 0u;
+            }
+#pragma unroll
+            for (u32 k = 0; k < 4; ++k) {
+                const bool hit = j + 8u * k + lg < len && test_bit(q.bm[y], x[k] - base_y);
+                c += __popc((__ballot_sync(FULL_MASK, hit) >> (grp * 8u)) & 0xffu);
+            }
         }
         if (r < R && lg == 0) q.P[r] = c;
     }
@@ -658,20 +682,25 @@ __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* ar
         group_label_run(g, r < R, v, d->label[y], s, e);
         const u32 base_y = r < R ? bucket_base(g, d->label[y]) : 0;
         u32 len = e - s, mx = warp_max(len), written = 0;
-        for (u32 j = 0; j < mx; j += 8) {
-            u32 pos = 0;
-            bool hit = false;
-            if (j + lg < len) {
-                pos = __ldg(g.nbr + s + j + lg) - base_y;
-                hit = test_bit(q.bm[y], pos);
+        for (u32 j = 0; j < mx; j += 32) {  // 4 loads in flight per lane, written in row order
+            u32 pos[4], word[4];
+#pragma unroll
+            for (u32 k = 0; k < 4; ++k) {
+                const u32 o = j + 8u * k + lg;
+                pos[k] = o < len ? __ldg(g.nbr + s + o) - base_y : 0u;
             }
-            u32 bal = (__ballot_sync(FULL_MASK, hit) >> (grp * 8u)) & 0xffu;
-            if (hit) {
-                u32 word = q.bm[y][pos >> 5];
-                u32 cpos = q.rank[y][pos >> 5] + __popc(word & ((1u << (pos & 31u)) - 1u));
-                q.adj[out + written + __popc(bal & ((1u << lg) - 1u))] = cpos;
+#pragma unroll
+            for (u32 k = 0; k < 4; ++k) word[k] = j + 8u * k + lg < len ? q.bm[y][pos[k] >> 5] : 0u;
+#pragma unroll
+            for (u32 k = 0; k < 4; ++k) {
+                const bool hit = (word[k] >> (pos[k] & 31u)) & 1u;
+                const u32 bal = (__ballot_sync(FULL_MASK, hit) >> (grp * 8u)) & 0xffu;
+                if (hit) {
+                    const u32 cpos = q.rank[y][pos[k] >> 5] + __popc(word[k] & ((1u << (pos[k] & 31u)) - 1u));
+                    q.adj[out + written + __popc(bal & ((1u << lg) - 1u))] = cpos;
+                }
+                written += __popc(bal);
             }
-            written += __popc(bal);
         }
     }
     TSYNC_B(t);
@@ -1336,7 +1365,7 @@ __global__ void __launch_bounds__(512) prep_cluster_kernel(DevGraph g, QState* q
 }
 
 // Plain path: one query prepared by the whole (co-resident) grid.
-__global__ void __launch_bounds__(512) prep_grid_kernel(DevGraph g, QState* qs, GridBarrier* bar, DevArena* arena,
+__global__ void __launch_bounds__(512, 1) prep_grid_kernel(DevGraph g, QState* qs, GridBarrier* bar, DevArena* arena,
                                                         u64 budget_ns) {
     GridTeam t{bar, global_timer_ns() + budget_ns};
     if (qs[0].step_cursor == HYBRID_REQUEST)
