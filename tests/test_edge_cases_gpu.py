@@ -65,3 +65,62 @@ def test_degenerate_graphs(engine, method):
         assert api.match(engine, dg, q, method).count == want, (g.num_vertices, q.num_vertices)
         assert api.match_batch(engine, dg, [q, q], method)[1].count == want
     assert api.match(engine, api.DataGraph.from_graph(g2), cases[3][1], method).count == 24
+
+
+def hub_graph():
+    """6,000 vertices, 6 labels, sparse random edges plus hub rows that put
+    label runs where row searches have their boundaries: one vertex adjacent
+    to all others (runs of about 1,000 entries), one whose whole row is one
+    label, one with runs of exactly 8 and 9 entries, and one adjacent only to
+    the last label."""
+    rng = np.random.default_rng(2024)
+    V, L = 6000, 6
+    lab = rng.integers(0, L, size=V).astype(np.uint32)
+    lab[:4] = [0, 1, 2, 3]
+    edges = set()
+    for v in range(1, V):
+        edges.add((0, v))
+    for v in np.flatnonzero(lab == 0):
+        if v > 3:
+            edges.add((1, int(v)))
+    for l, k in ((1, 8), (2, 9), (4, 1)):
+        for v in np.flatnonzero(lab == l)[:k + 4][-k:]:
+            if v > 3:
+                edges.add((2, int(v)))
+    for v in np.flatnonzero(lab == L - 1):
+        if v > 3:
+            edges.add((3, int(v)))
+    while len(edges) < 6000 + 20000:
+        a, b = (int(x) for x in rng.integers(4, V, size=2))
+        if a != b:
+            edges.add((min(a, b), max(a, b)))
+    return Graph.from_edges(V, lab, sorted(edges))
+
+
+def oracle_dump(r):
+    return {"cands": r.candidates, "tables": [(a, b, off, adj) for (a, b), (off, adj) in r.tables.items()],
+            "memory": r.memory_bytes, "order": list(r.order), "pivot": list(r.pivot)}
+
+
+def test_hub_rows_match_oracle(engine):
+    """Candidates, tables, orders and counts on hub rows (label runs of one
+    to thousands of entries, at the start, middle and end of a row) equal the
+    oracle's, under both methods."""
+    from tests.gpu_common import check_run_against_dump
+    g = hub_graph()
+    og = OracleGraph(g)
+    dg = api.DataGraph.from_graph(g)
+    qs = [Graph.from_edges(4, [0, 1, 2, 5], [(0, 1), (0, 2), (0, 3)]),          # star on the all-adjacent hub
+          Graph.from_edges(3, [1, 0, 0], [(0, 1), (0, 2)]),                     # the single-run row
+          Graph.from_edges(3, [2, 1, 2], [(0, 1), (0, 2), (1, 2)]),             # the 8 / 9-entry runs
+          Graph.from_edges(4, [3, 5, 5, 0], [(0, 1), (0, 2), (1, 3), (2, 3)])]  # the last label's run
+    qs += gen.make_queries(g, [3, 4, 5, 6, 8], gen.BASE_SEED + 31)
+    checked = 0
+    for q in qs:
+        for f, m in (("CFL", "CFL_CFL_EXPLORE"), ("GQL", "GQL_GQL_GQL")):
+            ref = og.run(q, f, f, cap=10**6)
+            with api.Run(engine, dg, q, m, cap=10**6) as run:
+                check_run_against_dump(run, oracle_dump(ref))
+                assert run.result.count == ref.count, (q.labels, m)
+            checked += 1
+    assert checked == 2 * len(qs)
