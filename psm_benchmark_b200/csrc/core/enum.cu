@@ -126,6 +126,7 @@ struct WarpStack {
     u32 cover;          // depths whose intersection overflowed CACHE_CAP for the current prefix
     u32 cbits;
     u32 cadj;
+    u32 near_q;         // query within reach of its cap: publish in small steps (~0: none)
     u32 pos[PSM_MAXQ];
     u32 vid[PSM_MAXQ];
     u32 cur[PSM_MAXQ];
@@ -975,9 +976,18 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
             }
         }
     }
-    if (count >= (1ull << 16) && lane == 0) {
+    // Far from the cap a warp publishes every 64 K embeddings. Once its own
+    // publish shows the query within reach of the cap (every warp's
+    // unpublished share, twice over, could cross it), it publishes every 1 K:
+    // the query then stops close to the cap instead of up to a share per warp
+    // beyond it. Only lane 0 reads and writes near_q.
+    if (lane == 0 && count >= (ws->near_q == qi ? (1ull << 10) : (1ull << 16))) {
         unsigned long long old = atomicAdd((unsigned long long*)&q.count, count);
-        if (q.cap && old + count >= q.cap) cap_reached(q);
+        if (q.cap) {
+            const u64 total = old + count;
+            if (total >= q.cap) cap_reached(q);
+            if (total + ((u64)(gridDim.x * (blockDim.x >> 5)) << 17) >= q.cap) ws->near_q = qi;
+        }
         count = 0;
     }
     count = __shfl_sync(FULL_MASK, count, 0);
@@ -1301,6 +1311,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 3) enum_kernel(DevGraph 
         ws->cover = 0;
         ws->cbits = 0;
         ws->cadj = 0;
+        ws->near_q = 0xFFFFFFFFu;
     }
     __syncwarp();
     TaskHdr t;
