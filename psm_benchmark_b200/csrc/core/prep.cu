@@ -489,11 +489,14 @@ __device__ bool step_generate(Team& t, const DevGraph& g, QState& q, u32 u, u32 
     const u32 base = bucket_base(g, lu), bsz = bucket_size(g, lu);
     const u32 per_blk = scan_block_words(W, t.nblocks());
     const u32 grp = lane >> 3, lg = lane & 7u;
+    const bool nlf_known = q.nlf_all;  // u's NLF set is in bm[u] (stage 1)
     for (u32 w = t.warp(); w < W; w += t.nwarps()) {
         u32 bits = q.acc[w];
         if (bsz - 32u * w < 32u) bits &= (1u << (bsz - 32u * w)) - 1u;  // W words cover bsz bits
         u32 word = 0;
-        if (__popc(bits) > 8u) {  // dense word: a lane per bit
+        if (nlf_known) {
+            word = bits & q.bm[u][w];
+        } else if (__popc(bits) > 8u) {  // dense word: a lane per bit
             const bool ok = ((bits >> lane) & 1u) && nlf_ok(g, d, u, base + 32u * w + lane);
             word = __ballot_sync(FULL_MASK, ok);
         } else {
@@ -1093,12 +1096,18 @@ __device__ bool run_step(Team& t, const DevGraph& g, QState& q, DevArena* arena,
         return true;
     }
     if (k == 1) {  // NLF candidates of the needed items
+        // CFL needs the NLF sets of its start options only. A team of >= 1024
+        // warps computes every vertex's set here, in one wide pass, and the
+        // generate steps then test a bit instead of walking NLF label runs
+        // (the sets are the same either way).
         u32 need = n >= 32 ? ~0u : ((1u << n) - 1u);
-        if (cfl) {
+        const bool all = !cfl || t.nwarps() >= 1024u;
+        if (!all) {
             need = 0;
             for (u32 j = 0; j < d->nfopt; ++j) need |= 1u << d->fopt_vertex[j];
         }
         stage_nlf(t, g, q, need, d->order == PSM_ORDER_CFL);
+        if (t.rank() == 0) q.nlf_all = all;
         TSYNC_B(t);
         return true;
     }

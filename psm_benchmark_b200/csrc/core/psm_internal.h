@@ -109,6 +109,7 @@ struct QState {
     u32 bwords[PSM_MAXQ];   // words per bitmap
     u32 cnt[PSM_MAXQ];      // candidate counts
     u32 item_cnt[PSM_MAXQ + PSM_MAXOPT];
+    u32 nlf_all;            // CFL: stage 1 left every vertex's NLF set in bm (large teams)
     u32* acc;               // CFL accumulator bitmap (max bwords)
     u32* tmp;               // CFL per-pivot bitmap
     u32 acc_words;          // words of acc / tmp
