@@ -55,32 +55,36 @@ __device__ __forceinline__ void label_run(const DevGraph& g, u32 v, u32 l, u32& 
     e = lower_bound_u32(g.nbr, s, hi, g.lab_off[l + 1]);
 }
 
-// lower_bound_u32 computed by the 8 lanes of an aligned lane group together:
-// each round probes 8 evenly spaced positions of the range (a 9-way split),
-// so a row of 1,000 entries takes 4 dependent loads instead of 10. Called
-// by the whole warp; lo, hi and key are uniform within each group, and a
-// group with lo == hi loads nothing.
+// lower_bound_u32 computed by the W (4 or 8) lanes of an aligned lane group
+// together: each round probes W evenly spaced positions of the range (a
+// (W + 1)-way split), so with W = 8 a row of 1,000 entries takes 4 dependent
+// loads instead of 10. Called by the whole warp; lo, hi and key are uniform
+// within each group, and a group with lo == hi loads nothing.
+template <u32 W = 8>
 __device__ __forceinline__ u32 group_lower_bound(const u32* __restrict__ a, u32 lo, u32 hi, u32 key) {
-    const u32 lg = lane_id() & 7u, sh = lane_id() & 24u;
-    while (__any_sync(FULL_MASK, hi - lo > 8u)) {
+    static_assert(W == 4 || W == 8, "group width");
+    constexpr u32 M = (1u << W) - 1u;
+    const u32 lg = lane_id() & (W - 1u), sh = lane_id() & ~(W - 1u);
+    while (__any_sync(FULL_MASK, hi - lo > W)) {
         const u32 n = hi - lo;
-        // probes lo + floor(n (j + 1) / 9), j = 0..7: distinct, inside (lo, hi)
+        // probes lo + floor(n (j + 1) / (W + 1)), j < W: distinct, inside (lo, hi)
         bool lt = false;
-        if (n > 8u) lt = __ldg(a + lo + (u32)((u64)n * (lg + 1u) / 9u)) < key;
-        const u32 c = __popc((__ballot_sync(FULL_MASK, lt) >> sh) & 0xffu);  // probes below key: a prefix
-        if (n > 8u) {
-            const u32 nlo = c ? lo + (u32)((u64)n * c / 9u) + 1u : lo;
-            const u32 nhi = c < 8u ? lo + (u32)((u64)n * (c + 1u) / 9u) : hi;
+        if (n > W) lt = __ldg(a + lo + (u32)((u64)n * (lg + 1u) / (W + 1u))) < key;
+        const u32 c = __popc((__ballot_sync(FULL_MASK, lt) >> sh) & M);  // probes below key: a prefix
+        if (n > W) {
+            const u32 nlo = c ? lo + (u32)((u64)n * c / (W + 1u)) + 1u : lo;
+            const u32 nhi = c < W ? lo + (u32)((u64)n * (c + 1u) / (W + 1u)) : hi;
             lo = nlo;
             hi = nhi;
         }
     }
     const bool lt = lg < hi - lo && __ldg(a + lo + lg) < key;
-    return lo + __popc((__ballot_sync(FULL_MASK, lt) >> sh) & 0xffu);
+    return lo + __popc((__ballot_sync(FULL_MASK, lt) >> sh) & M);
 }
 
-// label_run for the 8-lane group of this lane (v and l group-uniform; a
+// label_run for the W-lane group of this lane (v and l group-uniform; a
 // group with !valid gets an empty run). Called by the whole warp.
+template <u32 W = 8>
 __device__ __forceinline__ void group_label_run(const DevGraph& g, bool valid, u32 v, u32 l, u32& s, u32& e) {
     u32 lo = 0, hi = 0, k1 = 0, k2 = 0;
     if (valid && l < g.L) {
@@ -89,8 +93,8 @@ __device__ __forceinline__ void group_label_run(const DevGraph& g, bool valid, u
         k1 = g.lab_off[l];
         k2 = g.lab_off[l + 1];
     }
-    s = group_lower_bound(g.nbr, lo, hi, k1);
-    e = group_lower_bound(g.nbr, s, hi, k2);
+    s = group_lower_bound<W>(g.nbr, lo, hi, k1);
+    e = group_lower_bound<W>(g.nbr, s, hi, k2);
 }
 
 __device__ __forceinline__ bool test_bit(const u32* bm, u32 pos) { return (bm[pos >> 5] >> (pos & 31)) & 1u; }

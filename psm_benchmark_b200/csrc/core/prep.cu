@@ -25,7 +25,11 @@ namespace {
 
 // ---------------------------------------------------------------- teams --
 
+// kRowLanes: lanes per candidate row in the table passes. A small team keeps
+// more rows in flight with 4; the 148-block grid has rows enough and gains
+// from 8 on hub rows.
 struct BlockTeam {
+    static constexpr u32 kRowLanes = 4;
     __device__ u32 rank() const { return threadIdx.x; }
     __device__ u32 size() const { return blockDim.x; }
     __device__ u32 warp() const { return threadIdx.x >> 5; }
@@ -51,6 +55,7 @@ struct GridBarrier {
 // block raises `abort`, every later barrier returns false at once and the
 // kernel unwinds; the host reports an internal error.
 struct GridTeam {
+    static constexpr u32 kRowLanes = 8;
     GridBarrier* bar;
     u64 deadline_ns;
     __device__ u32 rank() const { return blockIdx.x * blockDim.x + threadIdx.x; }
@@ -95,6 +100,7 @@ struct GridTeam {
 // software barrier. Release/acquire at cluster scope makes the global-memory
 // writes of every block visible to the others after sync().
 struct ClusterTeam {
+    static constexpr u32 kRowLanes = 4;
     __device__ u32 rank() const { return cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
     __device__ u32 size() const { return cg::this_cluster().num_blocks() * blockDim.x; }
     __device__ u32 warp() const { return rank() >> 5; }
@@ -618,9 +624,11 @@ __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* ar
     }
     TSYNC_B(t);
     const u32 R = q.total_rows;
-    const u32 lane = lane_id(), grp = lane >> 3, lg = lane & 7u;
+    // Rows go to groups of TW lanes, 32 / TW rows per warp per round.
+    constexpr u32 TW = Team::kRowLanes, TG = 32 / TW, TM = (1u << TW) - 1u;
+    const u32 lane = lane_id(), grp = lane / TW, lg = lane % TW;
     // count pass
-    for (u32 r0 = t.warp() * 4u; r0 < R; r0 += t.nwarps() * 4u) {
+    for (u32 r0 = t.warp() * TG; r0 < R; r0 += t.nwarps() * TG) {
         u32 r = r0 + grp;
         u32 s, e, y = 0, v = 0;
         if (r < R) {
@@ -630,20 +638,20 @@ __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* ar
             y = d->e_dst[ei];
             v = q.list[x][i];
         }
-        group_label_run(g, r < R, v, d->label[y], s, e);
+        group_label_run<TW>(g, r < R, v, d->label[y], s, e);
         const u32 base_y = r < R ? bucket_base(g, d->label[y]) : 0;
         u32 len = e - s, mx = warp_max(len), c = 0;
-        for (u32 j = 0; j < mx; j += 32) {  // 4 loads in flight per lane
+        for (u32 j = 0; j < mx; j += 4u * TW) {  // 4 loads in flight per lane
             u32 x[4];
 #pragma unroll
             for (u32 k = 0; k < 4; ++k) {
-                const u32 o = j + 8u * k + lg;
+                const u32 o = j + TW * k + lg;
                 x[k] = o < len ? __ldg(g.nbr + s + o) : 0u;
             }
 #pragma unroll
             for (u32 k = 0; k < 4; ++k) {
-                const bool hit = j + 8u * k + lg < len && test_bit(q.bm[y], x[k] - base_y);
-                c += __popc((__ballot_sync(FULL_MASK, hit) >> (grp * 8u)) & 0xffu);
+                const bool hit = j + TW * k + lg < len && test_bit(q.bm[y], x[k] - base_y);
+                c += __popc((__ballot_sync(FULL_MASK, hit) >> (grp * TW)) & TM);
             }
         }
         if (r < R && lg == 0) q.P[r] = c;
@@ -671,7 +679,7 @@ __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* ar
     TSYNC_B(t);
     if (q.adj == nullptr) return true;
     // fill pass
-    for (u32 r0 = t.warp() * 4u; r0 < R; r0 += t.nwarps() * 4u) {
+    for (u32 r0 = t.warp() * TG; r0 < R; r0 += t.nwarps() * TG) {
         u32 r = r0 + grp;
         u32 s, e, y = 0, v = 0, out = 0;
         if (r < R) {
@@ -682,22 +690,22 @@ __device__ bool stage_tables(Team& t, const DevGraph& g, QState& q, DevArena* ar
             v = q.list[x][i];
             out = P[r];
         }
-        group_label_run(g, r < R, v, d->label[y], s, e);
+        group_label_run<TW>(g, r < R, v, d->label[y], s, e);
         const u32 base_y = r < R ? bucket_base(g, d->label[y]) : 0;
         u32 len = e - s, mx = warp_max(len), written = 0;
-        for (u32 j = 0; j < mx; j += 32) {  // 4 loads in flight per lane, written in row order
+        for (u32 j = 0; j < mx; j += 4u * TW) {  // 4 loads in flight per lane, written in row order
             u32 pos[4], word[4];
 #pragma unroll
             for (u32 k = 0; k < 4; ++k) {
-                const u32 o = j + 8u * k + lg;
+                const u32 o = j + TW * k + lg;
                 pos[k] = o < len ? __ldg(g.nbr + s + o) - base_y : 0u;
             }
 #pragma unroll
-            for (u32 k = 0; k < 4; ++k) word[k] = j + 8u * k + lg < len ? q.bm[y][pos[k] >> 5] : 0u;
+            for (u32 k = 0; k < 4; ++k) word[k] = j + TW * k + lg < len ? q.bm[y][pos[k] >> 5] : 0u;
 #pragma unroll
             for (u32 k = 0; k < 4; ++k) {
                 const bool hit = (word[k] >> (pos[k] & 31u)) & 1u;
-                const u32 bal = (__ballot_sync(FULL_MASK, hit) >> (grp * 8u)) & 0xffu;
+                const u32 bal = (__ballot_sync(FULL_MASK, hit) >> (grp * TW)) & TM;
                 if (hit) {
                     const u32 cpos = q.rank[y][pos[k] >> 5] + __popc(word[k] & ((1u << (pos[k] & 31u)) - 1u));
                     q.adj[out + written + __popc(bal & ((1u << lg) - 1u))] = cpos;
