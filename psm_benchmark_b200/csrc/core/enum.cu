@@ -103,12 +103,8 @@ constexpr u32 LONG_BM_ROW = 96;  // per-lane bitmap walks longer than this go to
 // With only `act` lanes holding a candidate, a lane's walk costs the warp its
 // whole length while the cooperative walk costs about 1/32 of it plus a fixed
 // setup: walks longer than these multiples of `act` go to the warp too.
-#ifndef PSM_DEFER_BM_K
-#define PSM_DEFER_BM_K 8
-#endif
-#ifndef PSM_DEFER_ROW_K
-#define PSM_DEFER_ROW_K 2
-#endif
+constexpr u32 DEFER_BM_PER_LANE = 8;
+constexpr u32 DEFER_ROW_PER_LANE = 2;
 
 // Invariants of the cache state: cvalid bit d => S of depth d is the
 // intersection for the current prefix; cbits bit d => the bitmap of depth d
@@ -545,8 +541,8 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
                                u64& calls, bool* defer, u32 act) {
     const u32 nb = q.nbn[dl];
     const u32 dp = dl - 1;
-    const u32 long_bm = min(LONG_BM_ROW, PSM_DEFER_BM_K * act);
-    const u32 long_row = min(LONG_ROW, max(2u, PSM_DEFER_ROW_K * act));
+    const u32 long_bm = min(LONG_BM_ROW, DEFER_BM_PER_LANE * act);
+    const u32 long_row = min(LONG_ROW, max(2u, DEFER_ROW_PER_LANE * act));
     if (cached) {
         const u32 s = ws->clen[dl];
         const u32 k = q.crow[dl];
