@@ -528,7 +528,11 @@ __device__ bool step_generate(Team& t, const DevGraph& g, QState& q, u32 u, u32 
 }
 
 // matching/FilterVertices.cpp:914-966 (pruneCandidates): keep a candidate of
-// u only if it is adjacent to a live candidate of every pivot.
+// u only if it is adjacent to a live candidate of every pivot. Only the bitmap
+// changes: u's list, rank and count stay those of its generation (a superset
+// whose dead entries have their bit clear), which every later filter step
+// reads through the bitmap, and the filter's last step compacts each pruned
+// vertex once.
 template <class Team>
 __device__ bool step_prune(Team& t, const DevGraph& g, QState& q, u32 u, u32 pivots) {
     const QDesc* d = q.desc;
@@ -538,7 +542,8 @@ __device__ bool step_prune(Team& t, const DevGraph& g, QState& q, u32 u, u32 piv
     for (u32 i0 = t.warp() * 4u; i0 < N; i0 += t.nwarps() * 4u) {
         u32 i = i0 + grp;
         u32 v = i < N ? q.list[u][i] : 0;
-        bool alive = i < N;
+        const bool live = i < N && test_bit(q.bm[u], v - base_u);  // the list may hold dead entries
+        bool alive = live;
         u32 pm = pivots;
         while (pm) {  // warp-uniform loop over pivots
             u32 p = __ffs(pm) - 1;
@@ -566,13 +571,11 @@ __device__ bool step_prune(Team& t, const DevGraph& g, QState& q, u32 u, u32 piv
             }
             if (alive && !found) alive = false;
         }
-        if (i < N && !alive && lg == 0) {
+        if (live && !alive && lg == 0) {
             u32 pos = v - base_u;
             atomicAnd(q.bm[u] + (pos >> 5), ~(1u << (pos & 31u)));
         }
     }
-    TSYNC_B(t);
-    if (!compact_vertex(t, g, q, u)) return false;
     TSYNC_B(t);
     return true;
 }
@@ -1209,6 +1212,18 @@ __device__ bool run_step(Team& t, const DevGraph& g, QState& q, DevArena* arena,
     }
     // tail: empty check, tables, order, enumeration plan
     if (j == 0) {
+        if (cfl) {  // lists of pruned vertices to their final sets
+            const FilterPlan& fp = d->fplan[q.froot];
+            u32 dirty = 0;
+            for (u32 s = 0; s < fp.nsteps; ++s)
+                if (fp.step_kind[s] == STEP_PRUNE) dirty |= 1u << fp.step_u[s];
+            while (dirty) {
+                const u32 u = __ffs(dirty) - 1;
+                dirty &= dirty - 1;
+                if (!compact_vertex(t, g, q, u)) return false;
+                TSYNC_B(t);  // the next scan reuses the scratch; the check below reads cnt
+            }
+        }
         if (t.rank() == 0)
             for (u32 u = 0; u < n; ++u)
                 if (q.cnt[u] == 0) q.empty = 1;
