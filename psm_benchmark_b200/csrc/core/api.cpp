@@ -157,7 +157,7 @@ int setup_query(psm_context* ctx, const psm_graph& g, const QDesc& d, const psm_
     q.tmp = b.take<u32>(maxw);
     q.acc_words = maxw;
     q.P = b.take<u32>(rows + 1);
-    q.scan = b.take<u32>(scan_words);
+    q.scan = b.take<u32>((size_t)scan_words * std::max(d.n, 1u));  // multi_compact: a block's word per vertex
     if (d.order == PSM_ORDER_CFL) {
         // one buffer pair per block that estimates paths concurrently
         q.est_blocks = std::max(1u, std::min(64u, scan_words - 1));

@@ -324,6 +324,70 @@ __device__ bool compact_vertex(Team& t, const DevGraph& g, QState& q, u32 u) {
         &q.cnt[u]);
 }
 
+// compact_vertex for every vertex in `mask` with one team barrier: a warp
+// per vertex sums the block's part of its bitmap into
+// scratch[k * nblocks + block] (k: the vertex's rank in mask; scratch holds
+// nblocks words per query vertex), then, after the barrier, adds the parts of
+// the blocks before it and emits the block's ranks and list entries. Same
+// word partition as team_scan. The caller syncs the team afterwards.
+template <class Team>
+__device__ bool multi_compact(Team& t, const DevGraph& g, QState& q, u32 mask) {
+    const u32 nb = t.nblocks(), b = t.block();
+    const u32 lane = lane_id(), w = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+    const u32 m = __popc(mask);
+    auto vertex = [&](u32 k) {
+        u32 x = mask;
+        for (u32 j = 0; j < k; ++j) x &= x - 1u;
+        return (u32)__ffs(x) - 1u;
+    };
+    for (u32 k = w; k < m; k += wpb) {
+        const u32 u = vertex(k), N = q.bwords[u];
+        const u32 per_blk = ((N + nb - 1) / nb + 31u) & ~31u;
+        const u32 b0 = min(N, b * per_blk), b1 = min(N, b0 + per_blk);
+        u32 c = 0;
+        for (u32 i = b0 + lane; i < b1; i += 32) c += __popc(q.bm[u][i]);
+        c = warp_sum(c);
+        if (lane == 0) q.scan[k * nb + b] = c;
+    }
+    TSYNC_B(t);
+    for (u32 k = w; k < m; k += wpb) {
+        const u32 u = vertex(k), N = q.bwords[u];
+        const u32 per_blk = ((N + nb - 1) / nb + 31u) & ~31u;
+        const u32 b0 = min(N, b * per_blk), b1 = min(N, b0 + per_blk);
+        u32 before = 0, all = 0;
+        for (u32 i = lane; i < nb; i += 32) {
+            const u32 v = ld_volatile_u32(q.scan + k * nb + i);
+            if (i < b) before += v;
+            all += v;
+        }
+        before = warp_sum(before);
+        all = warp_sum(all);
+        if (b == 0 && lane == 0) q.cnt[u] = all;
+        const u32* bm = q.bm[u];
+        u32* rank = q.rank[u];
+        u32* list = q.list[u];
+        const u32 base = bucket_base(g, q.desc->label[u]);
+        u32 carry = before;
+        for (u32 i0 = b0; i0 < b1; i0 += 32) {
+            const u32 i = i0 + lane;
+            u32 x = i < b1 ? bm[i] : 0u;
+            const u32 v = __popc(x);
+            const u32 incl = warp_incl_scan(v);
+            if (i < b1) {
+                u32 j = carry + incl - v;
+                rank[i] = j;
+                while (x) {
+                    const u32 bit = __ffs(x) - 1u;
+                    x &= x - 1u;
+                    list[j++] = base + 32u * i + bit;
+                }
+            }
+            carry += __shfl_sync(FULL_MASK, incl, 31);
+        }
+    }
+    return true;
+}
+
 // Stage 1: NLF candidates for every needed item, one warp per bitmap word.
 template <class Team>
 __device__ void stage_nlf(Team& t, const DevGraph& g, QState& q, u32 need_mask, bool want_virtual) {
@@ -1217,11 +1281,9 @@ __device__ bool run_step(Team& t, const DevGraph& g, QState& q, DevArena* arena,
             u32 dirty = 0;
             for (u32 s = 0; s < fp.nsteps; ++s)
                 if (fp.step_kind[s] == STEP_PRUNE) dirty |= 1u << fp.step_u[s];
-            while (dirty) {
-                const u32 u = __ffs(dirty) - 1;
-                dirty &= dirty - 1;
-                if (!compact_vertex(t, g, q, u)) return false;
-                TSYNC_B(t);  // the next scan reuses the scratch; the check below reads cnt
+            if (dirty) {
+                if (!multi_compact(t, g, q, dirty)) return false;
+                TSYNC_B(t);  // the check below reads cnt
             }
         }
         if (t.rank() == 0)

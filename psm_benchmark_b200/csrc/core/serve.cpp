@@ -96,7 +96,7 @@ u64 estimate_bytes(const psm_graph& g, const psm_query_desc& q, const psm_option
         maxb = std::max(maxb, B);
         rows += B * deg[u];
     }
-    b += 2 * al(4 * maxw) + al(4 * (rows + 1)) + al(8ull * (prep_blocks + 1));
+    b += 2 * al(4 * maxw) + al(4 * (rows + 1)) + al(4ull * (prep_blocks + 1) * std::max(n, 2u));
     if (opt.order == PSM_ORDER_CFL) b += al(8ull * 2 * prep_blocks * maxb) + al(8ull * PSM_PLAN_WORDS);
     for (u32 e = 0; e < q.num_edges; ++e) {
         const u32 la = q.labels[q.edges[2 * e]], lb = q.labels[q.edges[2 * e + 1]];
