@@ -272,8 +272,9 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     size_t desc_bytes = 0;
     for (u32 i = 0; i < nq; ++i) desc_bytes += align_up(psm_qdesc_bytes(descs[i]), 16);
     const size_t off_q = align_up(desc_bytes), off_a = off_q + align_up(sizeof(QState) * nq),
-                 off_r = off_a + align_up(sizeof(DevArena));
-    char* pin = staging(ctx, off_r + sizeof(DevResult) * nq);
+                 off_r = off_a + align_up(sizeof(DevArena)),
+                 off_c = off_r + align_up(sizeof(DevResult) * nq), off_b = off_c + align_up(psm_enum_ctl_bytes());
+    char* pin = staging(ctx, off_b + 16);
     if (!pin) return fail(PSM_ERR_OOM, "pinned host staging");
     {
         size_t o = 0;
@@ -324,17 +325,20 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     }
     std::vector<DevResult> res(nq);
     CK(cudaMemcpyAsync(pin + off_r, lay.d_res, sizeof(DevResult) * nq, cudaMemcpyDeviceToHost, ctx->st));
+    // the enumerator's control block and the grid barrier's abort word come
+    // back through the staging buffer too: one synchronisation per run
+    if (!prep_only) CK(psm_enum_copy_ctl(ctx->d_enum_scratch, pin + off_c, ctx->st));
+    if (grid_team)  // GridBarrier::abort (second word of the barrier)
+        CK(cudaMemcpyAsync(pin + off_b, (char*)ctx->d_barrier + 4, sizeof(u32), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
     EnumStats es{};
-    if (prep_only)
-        CK(cudaStreamSynchronize(ctx->st));
-    else
-        CK(psm_enum_read_ctl(ctx->d_enum_scratch, &es, ctx->st));  // synchronises the stream
+    if (!prep_only) psm_enum_ctl_stats(pin + off_c, &es);
     memcpy(res.data(), pin + off_r, sizeof(DevResult) * nq);
     const u32 enum_err = es.error;
     float prep_ms = 0, enum_ms = 0;
     CK(cudaEventElapsedTime(&prep_ms, ctx->ev[0], ctx->ev[1]));
     CK(cudaEventElapsedTime(&enum_ms, ctx->ev[1], ctx->ev[2]));
-    u64 h2d = sizeof(QState) * (u64)nq + sizeof(DevArena) + 64 + 4, d2h = sizeof(DevResult) * (u64)nq + 64;
+    u64 h2d = sizeof(QState) * (u64)nq + sizeof(DevArena) + 64 + 4, d2h = sizeof(DevResult) * (u64)nq + (prep_only ? 0 : psm_enum_ctl_bytes()) + (grid_team ? 4 : 0);
     for (u32 i = 0; i < nq; ++i) h2d += psm_qdesc_bytes(descs[i]);
     int worst = PSM_OK;
     for (u32 i = 0; i < nq; ++i) {
@@ -348,8 +352,7 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     }
     if (grid_team) {
         u32 ab = 0;
-        // GridBarrier::abort (second word of the barrier)
-        CK(cudaMemcpy(&ab, (char*)ctx->d_barrier + 4, sizeof(u32), cudaMemcpyDeviceToHost));
+        memcpy(&ab, pin + off_b, sizeof(u32));
         if (ab) {
             for (u32 i = 0; i < nq; ++i) results[i].status = PSM_ERR_INTERNAL;
             worst = PSM_ERR_INTERNAL;

@@ -1512,6 +1512,21 @@ cudaError_t psm_enum_max_blocks(int* blocks) {
 }
 
 // Reads back the launch-wide error flag and scheduling counters.
+size_t psm_enum_ctl_bytes() { return sizeof(EnumCtl); }
+
+cudaError_t psm_enum_copy_ctl(const void* scratch, void* host, cudaStream_t st) {
+    return cudaMemcpyAsync(host, scratch, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st);
+}
+
+void psm_enum_ctl_stats(const void* host, EnumStats* out) {
+    EnumCtl h;
+    memcpy(&h, host, sizeof(h));
+    out->error = h.error;
+    out->donations = h.donations;
+    out->tasks = h.tasks;
+    out->idle_polls = h.idle_polls;
+}
+
 cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st) {
     EnumCtl h;
     cudaError_t e = cudaMemcpyAsync(&h, scratch, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st);

@@ -96,5 +96,10 @@ cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch
 cudaError_t psm_enum_max_blocks(int* blocks);
 cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st);
 cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st);
+// Split form for callers with pinned staging: queue the control block's copy
+// on the stream, then read the stats once the stream has synchronised.
+size_t psm_enum_ctl_bytes();
+cudaError_t psm_enum_copy_ctl(const void* scratch, void* host, cudaStream_t st);
+void psm_enum_ctl_stats(const void* host, EnumStats* out);
 cudaError_t psm_launch_unit_plan(const DevGraph& g, QState* qs, u32 nq, cudaStream_t st);
 cudaError_t psm_launch_unit_emit(QState* qs, u32 nq, u32* const* bufs, const u64* caps, cudaStream_t st);
