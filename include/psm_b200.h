@@ -106,6 +106,15 @@ int psm_graph_store_binary(const uint32_t* offsets, const uint32_t* neighbors, c
 /* Text graph -> <prefix>_deg.bin, <prefix>_adj.bin, <prefix>_label.bin
  * (replaces matching/GraphConverter.cpp). Host only. */
 int psm_graph_convert(const char* text_path, const char* out_prefix);
+/* Edge list ("u v" per line, '#' comments) -> <prefix>_deg.bin, _adj.bin,
+ * _label.bin (replaces matching/EdgeListToCSR.cpp, run there as
+ * EdgeListConverter.out <edge list> <prefix> <number of labels>). Pairs are
+ * stored smaller id first and sorted; duplicates are kept; a self loop fails
+ * with nothing written. Labels are uniform over [0, num_labels) from
+ * std::mt19937 seeded with `seed` (the reference draws its seed from
+ * std::random_device). Host only. */
+int psm_graph_convert_edgelist(const char* edge_list_path, const char* out_prefix, uint32_t num_labels,
+                               uint64_t seed);
 int psm_graph_info(const psm_graph* g, uint32_t* num_vertices, uint64_t* num_edges, uint32_t* num_labels,
                    uint32_t* max_degree, uint32_t* max_label_frequency);
 void psm_graph_free(psm_graph* g);

@@ -394,3 +394,11 @@ def store_binary(g: Graph, prefix) -> None:
 def convert_text(text_path, prefix) -> None:
     """Text graph -> reference binary files (the reference's GraphConverter)."""
     N.check(N.lib().psm_graph_convert(str(text_path).encode(), str(prefix).encode()))
+
+
+def convert_edgelist(edge_list_path, prefix, num_labels: int, seed: int = 0) -> None:
+    """Edge list ("u v" per line) -> reference binary files (the reference's
+    EdgeListConverter), labels uniform over [0, num_labels) from a seeded
+    std::mt19937 (host only)."""
+    N.check(N.lib().psm_graph_convert_edgelist(str(edge_list_path).encode(), str(prefix).encode(),
+                                               int(num_labels), int(seed)))

@@ -23,6 +23,7 @@ int psm_graph_parse(const char* path, psm_graph** out, std::string* err);
 int psm_graph_parse_binary(const char* deg_path, const char* adj_path, const char* label_path, psm_graph** out,
                            std::string* err);
 int psm_text_to_binary(const char* text_path, const char* out_prefix, std::string* err);
+int psm_edgelist_to_binary(const char* path, const char* out_prefix, u32 num_labels, u64 seed, std::string* err);
 int psm_csr_write_binary(const u32* off, const u32* nbr, const u32* labels, u32 V, const char* deg_path,
                          const char* adj_path, const char* label_path, std::string* err);
 void psm_graph_destroy(psm_graph* g);
@@ -461,6 +462,14 @@ int psm_graph_convert(const char* text_path, const char* out_prefix) {
     if (!text_path || !out_prefix) return fail(PSM_ERR_ARG, "null argument");
     std::string err;
     int rc = psm_text_to_binary(text_path, out_prefix, &err);
+    return rc ? fail(rc, err) : PSM_OK;
+}
+
+int psm_graph_convert_edgelist(const char* edge_list_path, const char* out_prefix, uint32_t num_labels,
+                               uint64_t seed) {
+    if (!edge_list_path || !out_prefix) return fail(PSM_ERR_ARG, "null argument");
+    std::string err;
+    int rc = psm_edgelist_to_binary(edge_list_path, out_prefix, num_labels, seed, &err);
     return rc ? fail(rc, err) : PSM_OK;
 }
 

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -339,6 +340,92 @@ int psm_text_to_binary(const char* text_path, const char* out_prefix, std::strin
     if (rc) return rc;
     const std::string pre(out_prefix);
     return write_binary(h.off.data(), h.nbr.data(), h.labels.data(), h.V, (pre + "_deg.bin").c_str(),
+                        (pre + "_adj.bin").c_str(), (pre + "_label.bin").c_str(), err);
+}
+
+// Edge-list text -> the binary files above (matching/EdgeListToCSR.cpp, the
+// reference's EdgeListConverter). One "u v" pair of vertex ids per line;
+// lines starting with '#' and blank lines are skipped. Each pair is kept with
+// its smaller id first and the pairs are sorted. A self loop (v, v) fails the
+// whole conversion with nothing written (the reference prints "src >= dst"
+// and writes no files); duplicate pairs are kept, as there. |V| = largest id
+// + 1, |E| = number of pairs, and row v lists its neighbours in pair order:
+// those below v, then those above, each ascending. Labels are uniform over
+// [0, num_labels) from std::mt19937 seeded with `seed` (the reference seeds
+// it from std::random_device, so its labels change from run to run). As the
+// reference reads with getline until the stream is no longer good, a last
+// line without a newline is not used.
+int psm_edgelist_to_binary(const char* path, const char* out_prefix, u32 num_labels, u64 seed, std::string* err) {
+    if (num_labels == 0) {
+        *err = "number of labels must be positive";
+        return PSM_ERR_ARG;
+    }
+    FILE* f = fopen(path, "rb");
+    if (!f) {
+        *err = std::string("cannot open ") + path;
+        return PSM_ERR_IO;
+    }
+    std::string text;
+    char buf[1 << 16];
+    size_t got;
+    while ((got = fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, got);
+    fclose(f);
+    std::vector<std::pair<u32, u32>> pairs;
+    u64 max_id = 0;
+    bool any = false;
+    size_t line_no = 0;
+    for (size_t pos = 0;;) {
+        const size_t nl = text.find('\n', pos);
+        if (nl == std::string::npos) break;  // unterminated last line: not used
+        ++line_no;
+        const std::string line = text.substr(pos, nl - pos);
+        pos = nl + 1;
+        if (!line.empty() && line[0] == '#') continue;
+        const char* c = line.c_str();
+        while (*c == ' ' || *c == '\t' || *c == '\r') ++c;
+        if (*c == 0) continue;
+        char* end = nullptr;
+        long long ids[2];
+        bool ok = true;
+        for (int k = 0; k < 2 && ok; ++k) {
+            ids[k] = strtoll(c, &end, 10);
+            ok = end != c && ids[k] >= 0 && ids[k] < 0x7fffffffLL;
+            c = end;
+        }
+        if (!ok) {
+            *err = "line " + std::to_string(line_no) + ": expected two vertex ids in [0, 2^31 - 1)";
+            return PSM_ERR_ARG;
+        }
+        u32 a = (u32)ids[0], b = (u32)ids[1];
+        if (a > b) std::swap(a, b);
+        if (a == b) {
+            *err = "line " + std::to_string(line_no) + ": self loop (" + std::to_string(a) + ", " +
+                   std::to_string(b) + "); nothing written";
+            return PSM_ERR_ARG;
+        }
+        pairs.emplace_back(a, b);
+        max_id = std::max<u64>(max_id, b);
+        any = true;
+    }
+    std::sort(pairs.begin(), pairs.end());
+    const u32 V = any ? (u32)(max_id + 1) : 0u;
+    std::vector<u32> off(V + 1, 0);
+    for (const auto& e : pairs) {
+        off[e.first + 1]++;
+        off[e.second + 1]++;
+    }
+    for (u32 v = 0; v < V; ++v) off[v + 1] += off[v];
+    std::vector<u32> nbr(off[V]), fill(off.begin(), off.end() - 1);
+    for (const auto& e : pairs) {
+        nbr[fill[e.first]++] = e.second;
+        nbr[fill[e.second]++] = e.first;
+    }
+    std::vector<u32> labels(V);
+    std::mt19937 gen((std::mt19937::result_type)seed);
+    std::uniform_int_distribution<int> dis(0, (int)num_labels - 1);
+    for (u32 v = 0; v < V; ++v) labels[v] = (u32)dis(gen);
+    const std::string pre(out_prefix);
+    return write_binary(off.data(), nbr.data(), labels.data(), V, (pre + "_deg.bin").c_str(),
                         (pre + "_adj.bin").c_str(), (pre + "_label.bin").c_str(), err);
 }
 

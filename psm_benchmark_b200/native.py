@@ -28,7 +28,7 @@ EXPORTS = [
     "psm_match_join", "psm_query_decompose", "psm_hash_join",
     "psm_server_create", "psm_server_submit", "psm_server_poll", "psm_server_pending", "psm_server_estimate",
     "psm_server_clock_ns", "psm_server_destroy",
-    "psm_graph_load_binary", "psm_graph_store_binary", "psm_graph_convert",
+    "psm_graph_load_binary", "psm_graph_store_binary", "psm_graph_convert", "psm_graph_convert_edgelist",
 ]
 MAX_UNITS = 32
 
@@ -95,6 +95,7 @@ def lib():
         "psm_graph_load_binary": ([C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(vp)], C.c_int),
         "psm_graph_store_binary": ([u32p, u32p, u32p, C.c_uint32, C.c_char_p, C.c_char_p, C.c_char_p], C.c_int),
         "psm_graph_convert": ([C.c_char_p, C.c_char_p], C.c_int),
+        "psm_graph_convert_edgelist": ([C.c_char_p, C.c_char_p, C.c_uint32, C.c_uint64], C.c_int),
         "psm_graph_info": ([vp, u32p, C.POINTER(C.c_uint64), u32p, u32p, u32p], C.c_int),
         "psm_graph_free": ([vp], None),
         "psm_context_create": ([C.c_int, C.c_uint64, C.POINTER(vp)], C.c_int),

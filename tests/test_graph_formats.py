@@ -55,3 +55,53 @@ def test_binary_graph_matches_like_text(engine, tmp_path):
     dg = api.DataGraph.load_binary(tmp_path / "hprd")
     for q, c in zip(qs, counts):
         assert api.match(engine, dg, q, "CFL_CFL_EXPLORE").count == c
+
+
+EDGELIST_REF = __import__("pathlib").Path(__file__).resolve().parent / "golden" / "edgelist_ref.json"
+
+
+@pytest.mark.parametrize("name", ["basic", "random", "selfloop"])
+def test_edgelist_matches_the_reference_converter(tmp_path, name):
+    """Degree and adjacency files byte-identical to the reference's
+    EdgeListConverter (matching/EdgeListToCSR.cpp) on the recorded inputs
+    (tests/golden/make_edgelist_golden.py); a self loop writes nothing."""
+    import json
+    from psm_benchmark_b200.native import PsmError
+    rec = json.loads(EDGELIST_REF.read_text())[name]
+    src = tmp_path / "e.txt"
+    src.write_text(rec["text"])
+    pre = tmp_path / "g"
+    if not rec["written"]:
+        with pytest.raises(PsmError, match="self loop"):
+            api.convert_edgelist(src, pre, rec["num_labels"])
+        assert not list(tmp_path.glob("g_*"))
+        return
+    api.convert_edgelist(src, pre, rec["num_labels"], seed=3)
+    assert (tmp_path / "g_deg.bin").read_bytes() == bytes.fromhex(rec["deg"])
+    assert (tmp_path / "g_adj.bin").read_bytes() == bytes.fromhex(rec["adj"])
+    lab = np.fromfile(tmp_path / "g_label.bin", np.uint32)
+    assert lab.nbytes == rec["label_bytes"]
+    assert lab.max() < rec["num_labels"]
+
+
+def test_edgelist_labels_follow_the_seed(tmp_path):
+    src = tmp_path / "e.txt"
+    src.write_text("".join(f"{i} {i + 1}\n" for i in range(300)))
+    got = {}
+    for seed in (1, 1, 2):
+        api.convert_edgelist(src, tmp_path / f"s{seed}", 16, seed=seed)
+        lab = np.fromfile(tmp_path / f"s{seed}_label.bin", np.uint32)
+        assert lab.size == 301 and lab.max() < 16
+        assert seed not in got or np.array_equal(got[seed], lab)
+        got[seed] = lab
+    assert not np.array_equal(got[1], got[2])
+    assert len(np.unique(got[1])) > 8
+
+
+@pytest.mark.parametrize("text,labels", [("0 1\n2\n", 4), ("0 -1\n", 4), ("0 x\n", 4), ("0 1\n", 0)])
+def test_edgelist_rejects_malformed_input(tmp_path, text, labels):
+    from psm_benchmark_b200.native import PsmError
+    src = tmp_path / "e.txt"
+    src.write_text(text)
+    with pytest.raises(PsmError):
+        api.convert_edgelist(src, tmp_path / "g", labels)
