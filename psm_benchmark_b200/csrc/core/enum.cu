@@ -524,6 +524,8 @@ __device__ u64 emit_last(QState& q, const DevGraph& g, u32 d, WarpStack* ws, u64
 
 // Used same-label vertices (the lane's own v at depth dl - 1, the rest from
 // ws) whose position lies in S of dl and, when has_row, in R = adj[lo, hi).
+// R is then v's own row, which holds v only through a self loop: without
+// one, v is not looked up.
 __device__ __forceinline__ u32 cached_exclusions(const QState& q, u32 dl, u32 v, const WarpStack* ws, bool has_row,
                                                  u32 lo, u32 hi) {
     const u32 u = q.order[dl];
@@ -531,6 +533,7 @@ __device__ __forceinline__ u32 cached_exclusions(const QState& q, u32 dl, u32 v,
     u32 c = 0;
     for (u32 m = q.same_mask[dl]; m; m &= m - 1) {
         const u32 j = __ffs(m) - 1;
+        if (j == dp && has_row && !q.loops) continue;
         const u32 x = cand_pos(q, u, j == dp ? v : ws->vid[j]);
         if (x != 0xFFFFFFFFu && in_cache(q, ws, dl, x) && (!has_row || contains_u32(q.adj, lo, hi, x))) ++c;
     }
@@ -600,6 +603,8 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
     if (nb == 1) {
         u64 c = blen;
         u32 m = same;
+        // the row of v's own depth holds v only through a self loop
+        if (q.bn_depth[dl][0] == dp && !q.loops) m &= ~(1u << dp);
         while (m) {
             const u32 j = __ffs(m) - 1;
             m &= m - 1;

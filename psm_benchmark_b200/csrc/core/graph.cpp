@@ -66,6 +66,7 @@ int psm_graph_build(const uint32_t* off, const uint32_t* nbr, const uint32_t* la
         return PSM_ERR_ARG;
     }
     auto* g = new psm_graph;
+    g->dev.loops = 0;
     g->V = V;
     g->L = L;
     g->nnz = nnz;
@@ -105,6 +106,7 @@ int psm_graph_build(const uint32_t* off, const uint32_t* nbr, const uint32_t* la
                 return PSM_ERR_ARG;
             }
             dst[j] = g->to_internal[w];
+            if (w == v) g->dev.loops = 1;
         }
         std::sort(dst, dst + d);
     }

@@ -1067,8 +1067,9 @@ __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
     const u32 cm_l = __shfl_sync(FULL_MASK, cm, last), crow_l = __shfl_sync(FULL_MASK, crow, last);
     const u32 cnt_l = __shfl_sync(FULL_MASK, act ? q.cnt[u] : 0u, last);
     const u32 u_l = __shfl_sync(FULL_MASK, u, last);
-    const bool memo = n >= 3 && lane + 2 == n && crow == 0xFFFFFFFFu && cm_all != 0 && bm_ok && cm_l != 0 &&
-                      crow_l != 0xFFFFFFFFu && cnt_l <= PSM_MEMO_CAP;
+    // (the memo's exclusions assume a vertex is never its own neighbour)
+    const bool memo = !g.loops && n >= 3 && lane + 2 == n && crow == 0xFFFFFFFFu && cm_all != 0 && bm_ok &&
+                      cm_l != 0 && crow_l != 0xFFFFFFFFu && cnt_l <= PSM_MEMO_CAP;
     if (memo) cm = cm_all;
     const u32 memo_any = __ballot_sync(FULL_MASK, memo);
     u32 inval = 0;
@@ -1087,6 +1088,7 @@ __device__ void enum_plan_warp(const DevGraph& g, QState& q) {
     if (lane == 0) {
         q.bm_depths = bm_depths;
         q.memo_ok = memo_any ? 1u : 0u;
+        q.loops = g.loops;
     }
     if (memo) q.memo_tab = table_base(q, u_l, u);
     // memory cost: candidates of every vertex, both tables of every edge

@@ -36,6 +36,7 @@ struct DevGraph {
     const u32* nbr;      // [off[V]] internal ids
     const u32* lab_off;  // [L+1] bucket ranges
     const u32* orig;     // [V] internal -> original id
+    u32 loops;           // some vertex is its own neighbour (a self loop)
 };
 
 #ifndef PSM_B200_H
@@ -164,6 +165,7 @@ struct QState {
     // stays valid. memo_ok enables it; memo_tab = row base of T[u_l -> u_d].
     u32 memo_ok;
     u32 memo_tab;
+    u32 loops;              // the data graph has a self loop (DevGraph::loops)
     u32 root_cnt;
     // results
     u64 count;

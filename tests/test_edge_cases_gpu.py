@@ -124,3 +124,37 @@ def test_hub_rows_match_oracle(engine):
                 assert run.result.count == ref.count, (q.labels, m)
             checked += 1
     assert checked == 2 * len(qs)
+
+
+def with_self_loops(g, every=8):
+    """g with a self loop (v once in its own row) at every `every`-th vertex."""
+    V = g.num_vertices
+    rows = [list(g.neighbors(v)) for v in range(V)]
+    for v in range(0, V, every):
+        rows[v] = sorted(rows[v] + [v])
+    off = np.zeros(V + 1, np.uint32)
+    off[1:] = np.cumsum([len(r) for r in rows])
+    nbr = np.array([w for r in rows for w in r], np.uint32)
+    return Graph(off, nbr, np.asarray(g.labels, np.uint32))
+
+
+def test_self_loops_in_the_data_graph(engine):
+    """Self loops in the data graph: a vertex then sits in its own table rows
+    and passes filters it would fail without the loop, but no injective
+    embedding uses a loop. Counts equal the oracle's on the same graph and the
+    counts without the loops, plain and batched. Eight labels make
+    consecutive same-label depths common, where the enumerator's loop-free
+    shortcuts would otherwise apply; about half the queries finish below the
+    cap."""
+    base = gd.synthetic_graph("rmat12")
+    g0 = Graph(base.off, base.nbr, (np.asarray(base.labels) % 8).astype(np.uint32))
+    g1 = with_self_loops(g0)
+    og = OracleGraph(g1)
+    d0, d1 = api.DataGraph.from_graph(g0), api.DataGraph.from_graph(g1)
+    qs = gen.make_queries(g0, [4, 5, 6, 7, 8] * 3, gen.BASE_SEED + 41)
+    cap = 2000000
+    for f, m in (("CFL", "CFL_CFL_EXPLORE"), ("GQL", "GQL_GQL_GQL")):
+        want = [og.run(q, f, f, cap=cap, want_tables=False).count for q in qs]
+        assert [api.match(engine, d1, q, m, cap=cap).count for q in qs] == want
+        assert [api.match(engine, d0, q, m, cap=cap).count for q in qs] == want
+        assert [r.count for r in api.match_batch(engine, d1, qs, m, cap=cap)] == want
