@@ -79,6 +79,9 @@ typedef struct psm_result {
     uint64_t d2h_bytes;       /* device->host bytes of the call (its share)     */
     uint64_t tasks;           /* enumeration tasks run (launch-wide)            */
     uint64_t idle_polls;      /* polls of idle warps waiting for work           */
+    uint64_t count_internal;  /* embeddings the enumerator counted (unclamped:
+                                 >= count when the cap stopped the query; the
+                                 work and alg_bytes above correspond to it) */
 } psm_result;
 
 const char* psm_status_string(int status);
@@ -151,14 +154,16 @@ void psm_run_free(psm_run* run);
 
 /* No counterpart in the reference. Re-counts the embeddings of a prepared
  * run (psm_run_create with emit = 0) without allocating: for callers that
- * cannot allocate device memory at this point (inside CUDA stream capture,
- * latency-critical loops that cannot afford an allocation's implicit device
- * synchronisation, hosts whose device memory belongs to another runtime's
- * pool). The enumeration's scratch lives in a static 1 MiB device array per
- * GPU, held until process exit; the first call on a device looks up that
- * array's address, so make it before any stream capture. All calls share the
- * array: calls whose work overlaps on the GPU race and must not be issued.
- * Writes min(total, cap) to *count (cap 0 = none). */
+ * cannot allocate device memory at this point (serving loops that must not
+ * take an allocation's implicit device synchronisation, hosts whose device
+ * memory belongs to another runtime's pool). The enumeration's scratch lives
+ * in a static 1 MiB device array per GPU, held until process exit; the first
+ * call on a device looks up that array's address, so make it before any
+ * stream capture begins. The call runs on the run's context stream and waits
+ * for it. All calls share the array: calls whose work overlaps on the GPU
+ * race and must not be issued. A run whose preparation failed is refused with
+ * that status (PSM_ERR_OOM / _TIMEOUT / _INTERNAL). Writes min(total, cap) to
+ * *count (cap 0 = none). */
 int psm_run_recount_noalloc(psm_run* run, uint64_t cap, double time_limit_s, uint64_t* count, uint32_t* overtime);
 
 /* ---- decomposition + join path (replaces split_Q_test,

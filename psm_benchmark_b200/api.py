@@ -123,13 +123,15 @@ class MatchResult:
     d2h_bytes: int = 0
     tasks: int = 0
     idle_polls: int = 0
+    count_internal: int = 0  # unclamped count: the work alg_bytes covers
 
     @staticmethod
     def of(r: N.Result) -> "MatchResult":
         return MatchResult(count=r.count, calls=r.calls, memory_bytes=r.memory_bytes, table_entries=r.table_entries,
                            alg_bytes=r.alg_bytes, donations=r.donations, overtime=bool(r.overtime),
                            filter_ok=bool(r.filter_ok), status=r.status, prep_ms=r.prep_ms, enum_ms=r.enum_ms,
-                           h2d_bytes=r.h2d_bytes, d2h_bytes=r.d2h_bytes, tasks=r.tasks, idle_polls=r.idle_polls)
+                           h2d_bytes=r.h2d_bytes, d2h_bytes=r.d2h_bytes, tasks=r.tasks, idle_polls=r.idle_polls,
+                           count_internal=r.count_internal)
 
 
 def match(engine: Engine, data: DataGraph, query: Graph, method: str = "CFL_CFL_EXPLORE", cap: int = 0,

@@ -18,6 +18,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -68,7 +69,7 @@ def build_core(force: bool = False, verbose_ptxas: bool = False) -> Path:
         return out
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in CORE_CU:
         obj = objdir / (src.stem + ".cu.o")
         if force or _stale(obj, [src] + CORE_HDR + [INCLUDE / "psm_b200.h"]):
@@ -77,14 +78,18 @@ def build_core(force: bool = False, verbose_ptxas: bool = False) -> Path:
                    "-c", src, "-o", obj]
             if verbose_ptxas:
                 cmd[1:1] = ["-Xptxas", "-v"]
-            _run(cmd)
+            cmds.append(cmd)
         objs.append(obj)
     for src in CORE_CPP:
         obj = objdir / (src.stem + ".cpp.o")
         if force or _stale(obj, [src] + CORE_HDR + [INCLUDE / "psm_b200.h"]):
-            _run([CXX, "-std=c++17", "-O3", "-fPIC", "-pthread", f"-I{INCLUDE}", f"-I{CSRC / 'core'}",
-                  f"-I{CUDA_HOME / 'include'}", "-c", src, "-o", obj])
+            cmds.append([CXX, "-std=c++17", "-O3", "-fPIC", "-pthread", f"-I{INCLUDE}", f"-I{CSRC / 'core'}",
+                         f"-I{CUDA_HOME / 'include'}", "-c", src, "-o", obj])
         objs.append(obj)
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(_run, c) for c in cmds]:
+            f.result()
     _run([NVCC, *GENCODE, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", out,
           "-lcudart", "-lpthread"])
     return out

@@ -122,6 +122,7 @@ int psm_run_internals(psm_run* r, RunInternals* out) {
     out->dev = &r->g->dev;
     out->enum_blocks = r->ctx->enum_blocks;
     out->emit = r->hq.emit_buf != nullptr;
+    out->prep_status = r->hq.status;
     return PSM_OK;
 }
 
@@ -196,6 +197,7 @@ u64 budget_ns(const psm_options& o) {
 
 void fill_result(const DevResult& r, float prep_ms, float enum_ms, u64 donations, psm_result* out) {
     out->count = r.count;
+    out->count_internal = r.count_internal;
     out->calls = r.calls;
     out->memory_bytes = r.memory_bytes;
     out->table_entries = r.table_nnz;

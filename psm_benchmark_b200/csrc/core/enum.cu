@@ -1453,6 +1453,7 @@ __global__ void gather_kernel(const QState* qs, u32 nq, DevResult* out) {
         const QState& q = qs[i];
         DevResult r;
         r.count = q.cap && q.count > q.cap ? q.cap : q.count;
+        r.count_internal = q.count;
         r.calls = q.calls;
         r.alg_bytes = q.alg_bytes;
         r.memory_bytes = q.memory_bytes;
@@ -1516,13 +1517,15 @@ cudaError_t psm_enum_max_blocks(int* blocks) {
     return cudaSuccess;
 }
 
-// Reads back the launch-wide error flag and scheduling counters.
+// Size of the launch-wide control block (error flag, scheduling counters).
 size_t psm_enum_ctl_bytes() { return sizeof(EnumCtl); }
 
+// Queues a copy of the control block into host memory (pinned staging).
 cudaError_t psm_enum_copy_ctl(const void* scratch, void* host, cudaStream_t st) {
     return cudaMemcpyAsync(host, scratch, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st);
 }
 
+// Decodes a control block copied by psm_enum_copy_ctl.
 void psm_enum_ctl_stats(const void* host, EnumStats* out) {
     EnumCtl h;
     memcpy(&h, host, sizeof(h));
@@ -1532,6 +1535,7 @@ void psm_enum_ctl_stats(const void* host, EnumStats* out) {
     out->idle_polls = h.idle_polls;
 }
 
+// Reads back the launch-wide error flag and scheduling counters.
 cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st) {
     EnumCtl h;
     cudaError_t e = cudaMemcpyAsync(&h, scratch, sizeof(EnumCtl), cudaMemcpyDeviceToHost, st);

@@ -46,6 +46,7 @@ struct RunInternals {
     const DevGraph* dev;
     int enum_blocks;
     u32 emit;
+    u32 prep_status;  // PSM_DEV_* status the run's preparation ended with
 };
 int psm_run_internals(psm_run* run, RunInternals* out);
 

@@ -190,6 +190,7 @@ struct QState {
 // Compact per-query result gathered after enumeration.
 struct DevResult {
     u64 count, calls, alg_bytes, memory_bytes, table_nnz, emit_rows;
+    u64 count_internal;  // unclamped count (work done before the stop)
     u32 status, overtime, filter_ok, empty;
 };
 

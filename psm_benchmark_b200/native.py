@@ -55,7 +55,7 @@ class Result(C.Structure):
                 ("overtime", C.c_uint32), ("filter_ok", C.c_uint32), ("status", C.c_uint32),
                 ("reserved", C.c_uint32), ("prep_ms", C.c_double), ("enum_ms", C.c_double),
                 ("h2d_bytes", C.c_uint64), ("d2h_bytes", C.c_uint64), ("tasks", C.c_uint64),
-                ("idle_polls", C.c_uint64)]
+                ("idle_polls", C.c_uint64), ("count_internal", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

@@ -156,3 +156,31 @@ def test_algorithmic_bytes_match_oracle(engine):
             assert got.count == ref.count
             if not entry["cap"] or ref.count < entry["cap"]:
                 assert got.alg_bytes == int(ref.depth_bytes.sum()), (m, q.num_vertices)
+
+
+def test_algorithmic_bytes_of_capped_queries(engine):
+    """A capped query stops part-way through the search tree. Its bytes and
+    its unclamped count (count_internal) come from the same extended partial
+    embeddings, so: count_internal lies between the cap and the full count,
+    and the bytes are at most the full tree's bytes (the oracle's exact
+    figure), also after scaling them to the cap (bytes x cap / count_internal,
+    the numerator of the bench's roofline)."""
+    g, qs, counts = gd.hprd()
+    og = OracleGraph(g)
+    dg = api.DataGraph.from_graph(g)
+    checked = 0
+    for q in qs:
+        full = og.run(q, "CFL", "CFL", want_tables=False)
+        full_bytes = int(full.depth_bytes.sum())
+        if full.count < 30:
+            continue
+        for cap in (full.count // 3, full.count - 1):
+            got = api.match(engine, dg, q, "CFL_CFL_EXPLORE", cap=cap)
+            assert got.count == cap
+            assert cap <= got.count_internal <= full.count
+            assert got.alg_bytes <= full_bytes
+            assert got.alg_bytes * cap / got.count_internal <= full_bytes
+            checked += 1
+        got = api.match(engine, dg, q, "CFL_CFL_EXPLORE")
+        assert got.count_internal == got.count == full.count
+    assert checked >= 4

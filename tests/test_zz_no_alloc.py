@@ -53,3 +53,53 @@ def test_recount_noalloc_rejects_emit_runs():
             rc = N.lib().psm_run_recount_noalloc(run._h, 0, 60.0, C.byref(cnt), None)
             assert rc == N.PSM_ERR_ARG
         dg.close()
+
+
+def _kept_failed_run(dg, q):
+    """A run whose preparation failed on the device (its candidate tables did
+    not fit the arena) but whose handle psm_run_create kept. Found by
+    bisecting the context's arena size between a size where the host-side
+    setup already fails and one where the query runs."""
+    qb = api._QueryBuf(q)
+    opt = api.options("CFL_CFL_EXPLORE", 0, 60.0, 0)
+    lo, hi = 1 << 20, 1 << 30
+    for _ in range(40):
+        size = (lo + hi) // 2
+        try:
+            eng = api.Engine(arena_bytes=size)
+        except N.PsmError:  # smaller than the context's fixed region
+            lo = size
+            continue
+        h = C.c_void_p()
+        res = N.Result()
+        rc = N.lib().psm_run_create(eng._h, dg._h, C.byref(qb.desc), C.byref(opt), C.byref(h), C.byref(res))
+        if rc == N.PSM_OK:
+            N.lib().psm_run_free(h)
+            eng.close()
+            hi = size
+        elif rc == N.PSM_ERR_OOM and not h.value:
+            eng.close()
+            lo = size
+        else:
+            assert rc == N.PSM_ERR_OOM, rc
+            return eng, h
+        if hi - lo <= 64:
+            break
+    pytest.fail("no arena size left the run's preparation out of memory")
+
+
+def test_recount_noalloc_refuses_failed_preparation():
+    g = gd.synthetic_graph("rmat12")
+    case = dict(gd.synthetic_cases())["rmat12"]
+    q = gd.query_from_rec(case["queries"][0]["query"])
+    dg = api.DataGraph.from_graph(g)
+    eng, h = _kept_failed_run(dg, q)
+    try:
+        cnt = C.c_uint64(7)
+        rc = N.lib().psm_run_recount_noalloc(h, 0, 60.0, C.byref(cnt), None)
+        assert rc == N.PSM_ERR_OOM, N.lib().psm_last_error()
+        assert cnt.value == 7  # nothing written on refusal
+    finally:
+        N.lib().psm_run_free(h)
+        eng.close()
+        dg.close()
