@@ -14,15 +14,22 @@ from the device time of the launches (CUDA events on the library's stream,
 graph resident in HBM); `e2e` is the same through the C ABI call psm_match
 with host query buffers, host->device descriptor copies (through the
 context's pinned staging buffer) and device->host result reads inside the
-wall-clock timed region. The data graph (72 MB) fits
-in L2, so L2 is flushed (256 MiB write) before every timed step. With N GPUs
-each rank runs the whole workload on its own replica of the graph (replicas
-only, weak scaling); times are the max over ranks.
+wall-clock timed region. The data graph (72 MB) fits in L2, so L2 is flushed
+(256 MiB write) before every timed step. With N GPUs each rank runs the whole
+workload on its own replica of the graph (replicas only, weak scaling); times
+are the max over ranks.
+
+At N=1 the same line also carries the other workloads of the path:
+`batched_mixed` (2,000 queries of 4-32 vertices on the same graph, batched vs
+plain, counts equal), `serve` (R-MAT scale 24, a 50,000-request Poisson
+stream at 50/80/95 % of saturation, p50/p99) and `cpu_baseline` (the
+reference binary on the host cores, whole queries, counts compared).
 
 --impl reference times the reference's own CPU implementation (the
 SubgraphMatching.out binary built from the reference sources by
-oracle/Makefile) on the host cores, per query with -threadnums = all cores,
-on a bounded sample of the same queries per step.
+oracle/Makefile) on the host cores: one step is one whole query of the same
+workload run to its end (count = min(total, 1e9), Overtime: 0), and the steps
+run as concurrent reference processes, one per host thread.
 """
 from __future__ import annotations
 
@@ -35,6 +42,7 @@ import sys
 import tempfile
 import threading
 import time
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 import numpy as np
@@ -45,13 +53,14 @@ sys.path.insert(0, str(ROOT))
 METRIC = "queries/sec (plain GPU path, CFL_CFL_EXPLORE, cap 1e9)"
 WORKLOAD = "plain_rmat_s20"
 REF_BIN = ROOT / "oracle" / "_ref" / "SubgraphMatching.out"
-# The reference counts a capped query exactly only with one thread: with more
-# threads every task counts up to the cap on its own (EvaluateQuery.cpp:
-# 137,152) and the run overshoots the 1e9 cap (about 4e9 counted after 30 s
-# on 8 threads here) until its time limit ends it.
-REF_THREADS = 1
-REF_THREADS_NOTE = ("-threadnums 1: multi-threaded reference runs of capped queries overshoot the cap and run "
-                    "until the time limit, so one thread is the reference's fastest exact configuration")
+# The reference counts a capped query exactly only with one thread per
+# process: with more threads every task counts up to the cap on its own
+# (EvaluateQuery.cpp:137,152), so a multi-threaded run of a capped query
+# overshoots the cap (4.4e9 counted in 30 s on 8 threads) and runs until its
+# time limit. The host's threads are therefore used as concurrent one-thread
+# processes, one query each; one multi-threaded run is reported beside them.
+REF_NOTE = ("whole queries, one reference process per host thread, -threadnums 1 each: a multi-threaded "
+            "reference run of a capped query overshoots the cap and runs until its time limit (see 'multithread')")
 
 
 def enum_traffic():
@@ -131,20 +140,32 @@ def make_workload(args):
     return w
 
 
+def workload_config(w, world):
+    """The `config` object of both arms (same workload, same keys)."""
+    sizes = sorted({q.num_vertices for q in w.queries})
+    return {"workload": WORKLOAD, "graph": f"R-MAT scale {int(np.log2(w.graph.num_vertices))}, edge factor 8, "
+                                          "32 uniform labels",
+            "vertices": w.graph.num_vertices, "edges": w.graph.num_edges, "queries_per_step": len(w.queries),
+            "query_sizes": " + ".join(f"{sum(q.num_vertices == k for q in w.queries)} x {k}" for k in sizes),
+            "method": w.method, "cap": w.cap, "parallelism": f"replicas x{world}",
+            "l2": "flushed (256 MiB write) before every step; 72 MB graph L2-resident within a step"}
+
+
 # --------------------------------------------------------------- reference --
 
 def ref_available():
     return REF_BIN.exists() and os.access(REF_BIN, os.X_OK)
 
 
-def run_reference_query(data_txt, qpath, threads, cap, tmp: Path, time_limit=600):
-    log = tmp / "ref.log"
+def run_reference_query(data_txt, qpath, threads, cap, log: Path, time_limit=600):
+    """One SubgraphMatching.out run in -QorCandi C mode; returns (Total time,
+    #Embeddings, Overtime) from its log block."""
     if log.exists():
         log.unlink()
     cmd = [str(REF_BIN), "-d", data_txt, "-q", qpath, "-threadnums", str(threads),
-           "-num", str(cap) if cap else "MAX", "-time_limit", str(time_limit), "-OutputFile", str(log),
+           "-num", str(cap) if cap else "MAX", "-time_limit", str(int(time_limit)), "-OutputFile", str(log),
            "-QorCandi", "C", "-split", "linear", "-schedule", "busy2idlenostop", "-BackMethods", "CFL_CFL_EXPLORE"]
-    subprocess.run(cmd, check=True, capture_output=True, timeout=time_limit + 120)
+    subprocess.run(cmd, check=True, capture_output=True, timeout=time_limit + 300)
     text = log.read_text()
     total = float(re.findall(r"Total time \(seconds\): ([0-9.e+-]+)", text)[-1])
     count = int(re.findall(r"#Embeddings: (\d+)", text)[-1])
@@ -152,9 +173,13 @@ def run_reference_query(data_txt, qpath, threads, cap, tmp: Path, time_limit=600
     return total, count, over
 
 
+def ref_workers():
+    return max(1, os.cpu_count() or 1)
+
+
 class ReferenceRunner:
     """Writes the workload in the reference's text format once and runs the
-    reference binary per query."""
+    reference binary on its queries, as concurrent one-query processes."""
 
     def __init__(self, w):
         from psm_benchmark_b200 import gen
@@ -172,25 +197,35 @@ class ReferenceRunner:
             self.qpaths.append(str(p))
         self.cap = w.cap
 
-    def sample(self, threads, budget_s, start=0, cap=None):
-        """Runs queries from `start` (cyclic) until `budget_s` seconds of
-        reference "Total time" have accumulated. Each run gets the remaining
-        budget as its -time_limit, so the sample stays bounded; a run that
-        hits the limit contributes the fraction of its query it finished
-        (embeddings counted / cap). Returns (query_equivalents, total_s,
-        [(count, overtime)])."""
-        cap = self.cap if cap is None else cap
-        qeq, tot, runs = 0.0, 0.0, []
-        i = start
-        while tot < budget_s and len(runs) < len(self.qpaths):
-            limit = max(1, int(round(budget_s - tot)))
-            t, c, over = run_reference_query(self.data_txt, self.qpaths[i % len(self.qpaths)], threads, cap,
-                                             self.tmp, time_limit=limit)
-            qeq += (min(c, cap) / cap) if cap else (0.0 if over else 1.0)
-            tot += t
-            runs.append((c, over))
-            i += 1
-        return qeq, tot, runs
+    def pool(self, indices, workers, threads=1, time_limit=600):
+        """Runs the queries `indices` (one process each, `threads` threads per
+        process) on `workers` concurrent slots. Returns the runs as
+        (query index, slot, total_s, count, overtime), the makespan over
+        slots of the reference's own Total time (graph loading excluded, as
+        in the reference's log) and the wall time."""
+        lock = threading.Lock()
+        slots = {}
+        runs = []
+
+        def one(i):
+            tid = threading.get_ident()
+            with lock:
+                slot = slots.setdefault(tid, len(slots))
+            log = self.tmp / f"log_{slot}.txt"
+            t, c, over = run_reference_query(self.data_txt, self.qpaths[i % len(self.qpaths)], threads, self.cap,
+                                             log, time_limit)
+            with lock:
+                runs.append((i, slot, t, c, over))
+
+        t0 = time.time()
+        with ThreadPoolExecutor(max_workers=workers) as ex:
+            for f in [ex.submit(one, i) for i in indices]:
+                f.result()
+        wall = time.time() - t0
+        per_slot = {}
+        for _, slot, t, _, _ in runs:
+            per_slot[slot] = per_slot.get(slot, 0.0) + t
+        return sorted(runs), max(per_slot.values()), wall
 
 
 def cpu_info():
@@ -203,6 +238,15 @@ def cpu_info():
     return "unknown"
 
 
+def reference_multithread(rr, threads, limit):
+    """One run of query 0 with the reference's own multi-threaded engine."""
+    t, c, over = run_reference_query(rr.data_txt, rr.qpaths[0], threads, rr.cap, rr.tmp / "log_mt.txt", limit)
+    return {"threads": threads, "time_limit_s": limit, "total_s": t, "embeddings": c, "overtime": over,
+            "reached_cap": bool(rr.cap and c >= rr.cap), "embeddings_per_s": c / t if t > 0 else None,
+            "note": "one query, -threadnums = host threads; a capped query overshoots the cap (tasks count to the "
+                    "cap independently, EvaluateQuery.cpp:137,152) and stops only at the time limit"}
+
+
 def reference_arm(args, world, rank):
     if rank != 0:
         return
@@ -212,32 +256,28 @@ def reference_arm(args, world, rank):
         return
     w = make_workload(args)
     rr = ReferenceRunner(w)
-    cores = REF_THREADS
-    for i in range(args.warmup):
-        rr.sample(cores, 0.5, start=i, cap=100000)
-    q_tot, t_tot = 0.0, 0.0
-    nq = 0
-    t0 = time.time()
-    for s in range(args.steps):
-        qeq, tot, runs = rr.sample(cores, args.ref_budget, start=s * 7)
-        q_tot += qeq
-        t_tot += tot
-        nq += len(runs)
-    wall = time.time() - t0
-    sec_per_query = t_tot / max(q_tot, 1e-12)
-    value = q_tot / t_tot
+    workers = ref_workers()
+    nq = len(w.queries)
+    # warm-up: the graph file and the binary into the page cache
+    rr.pool([nq - 1 - i for i in range(args.warmup)], workers, time_limit=1)
+    runs, makespan, wall = rr.pool(list(range(args.steps)), workers, time_limit=args.ref_limit)
+    over = sum(r[4] for r in runs)
+    value = len(runs) / makespan
+    mt = reference_multithread(rr, workers, args.ref_mt_limit) if args.ref_mt_limit > 0 else None
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_query * 1e3 * len(w.queries),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": makespan * 1e3 / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "queries_per_step": len(w.queries), "method": "CFL_CFL_EXPLORE",
-                       "cap": w.cap},
-            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": cores, "kind": "reference",
-                             "sample": f"{nq} query runs over {args.steps} steps, {args.ref_budget:.0f} s of "
-                                       f"reference Total time per step, {q_tot:.3f} query-equivalents counted "
-                                       f"(embeddings counted / 1e9 cap), -threadnums {cores}, CPU {cpu_info()} "
+            "config": workload_config(w, args.gpus),
+            "cpu_baseline": {"value": value, "unit": "queries/s", "cores": workers, "kind": "reference",
+                             "sample": f"{len(runs)} whole queries (workload queries 0-{len(runs) - 1}), one per step, "
+                                       f"on {workers} concurrent one-thread reference processes; value = queries / "
+                                       f"makespan of the reference's Total time ({makespan:.1f} s; wall with graph "
+                                       f"loading {wall:.1f} s); {over} run(s) hit the time limit; CPU {cpu_info()} "
                                        f"({os.cpu_count()} threads)",
-                             "wall_s": wall, "note": REF_THREADS_NOTE},
+                             "counts": [r[3] for r in runs], "wall_s": wall, "note": REF_NOTE},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if mt is not None:
+        line["multithread"] = mt
     print(json.dumps(line))
 
 
@@ -245,6 +285,37 @@ def reference_arm(args, world, rank):
 
 def flush_l2(buf):
     buf.add_(1)
+
+
+def scaled_bytes(r, cap):
+    """Algorithmic bytes of a query, scaled to the cap when the enumerator
+    counted past it before the stop reached every warp: bytes and the
+    unclamped count come from the same extended partial embeddings, so
+    bytes x cap / count_internal is the work of `cap` embeddings at the
+    query's own bytes per embedding."""
+    if cap and r.count_internal > cap:
+        return r.alg_bytes * cap / r.count_internal
+    return float(r.alg_bytes)
+
+
+def cpu_baseline(w, counts, n):
+    """The reference binary on the host cores: n whole queries of the
+    workload (queries 0..n-1), concurrent one-thread processes, counts
+    compared with this arm's."""
+    rr = ReferenceRunner(w)
+    runs, makespan, wall = rr.pool(list(range(n)), ref_workers())
+    checked = 0
+    for i, _, _, c, over in runs:
+        if not over:
+            if c != counts[i]:
+                raise SystemExit(f"reference count {c} differs from ours {counts[i]} (query {i})")
+            checked += 1
+    return {"value": len(runs) / makespan, "unit": "queries/s", "cores": min(ref_workers(), n), "kind": "reference",
+            "sample": f"{len(runs)} whole queries (workload queries 0-{len(runs) - 1}) on {min(ref_workers(), n)} "
+                      f"concurrent one-thread reference processes; value = queries / makespan of the reference's "
+                      f"Total time ({makespan:.1f} s; wall with graph loading {wall:.1f} s); CPU {cpu_info()} "
+                      f"({os.cpu_count()} threads)",
+            "reference_counts_checked": checked, "note": REF_NOTE}
 
 
 def ours_arm(args, world, rank, local):
@@ -282,10 +353,11 @@ def ours_arm(args, world, rank, local):
     barrier()
     dev_ms = 0.0
     enum_ms = 0.0
-    alg = 0
+    alg = 0.0
     lat = []
     h2d = d2h = 0
     counts = None
+    internal = 0
     t0 = time.perf_counter()
     for s in range(args.steps):
         flush_l2(flush)
@@ -294,7 +366,8 @@ def ours_arm(args, world, rank, local):
         dev_ms += sum(r.prep_ms + r.enum_ms for r in res)
         lat += [r.prep_ms + r.enum_ms for r in res]
         enum_ms += sum(r.enum_ms for r in res)
-        alg += sum(r.alg_bytes for r in res)
+        alg += sum(scaled_bytes(r, w.cap) for r in res)
+        internal += sum(r.count_internal for r in res)
         h2d += sum(r.h2d_bytes for r in res)
         d2h += sum(r.d2h_bytes for r in res)
         counts = [r.count for r in res]
@@ -313,25 +386,23 @@ def ours_arm(args, world, rank, local):
     achieved = alg / (enum_ms / 1e3) / 1e9 if enum_ms > 0 else 0.0
     line = {"metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "graph": "R-MAT scale 20, edge factor 8, 32 uniform labels",
-                       "vertices": w.graph.num_vertices, "edges": w.graph.num_edges,
-                       "queries_per_step": nq, "query_sizes": "100 x 12, 100 x 16", "method": w.method,
-                       "cap": w.cap, "parallelism": f"replicas x{world}",
-                       "l2": "flushed (256 MiB write) before every step; 72 MB graph L2-resident within a step"},
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": workload_config(w, world),
             "embeddings_per_s": world * sum(counts) * args.steps / (dev_ms / 1e3),
             # per-query device latency of the plain path (preparation + enumeration)
             "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                            "max": float(max(lat))},
             "e2e": {"value": e2e, "unit": "queries/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
-            # per plain-path query: prep, enum-init, enum, gather kernels + 2 memsets
+            # per plain-path query: prep, enum-init, enum, gather kernels
             "gpu_launches": 4 * nq * args.steps,
             "roofline": {"bound": "hbm", "kernel": "enum_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "peak_kind": peak_kind,
                          # ncu DRAM bytes per launch (profiles/) against the
                          # algorithmic bytes per launch of this run
-                         "traffic": enum_traffic(), "alg_bytes_per_launch": alg / (nq * args.steps)},
+                         "traffic": enum_traffic(), "alg_bytes_per_launch": alg / (nq * args.steps),
+                         "numerator": "reference-equivalent intersection bytes, scaled to the cap on queries "
+                                      "counted past it (bytes x cap / unclamped count)",
+                         "counted_past_cap": internal / max(1, sum(counts) * args.steps) - 1.0},
             "clocks": clk}
     # Batched path on the same queries: one preparation launch + one
     # enumeration launch for the whole step (device time, CUDA events).
@@ -350,17 +421,13 @@ def ours_arm(args, world, rank, local):
         bval = world * nq * args.steps / (bt / 1e3)
         line["batched"] = {"value": bval, "unit": "queries/s", "ms_per_step": bt / args.steps,
                            "speedup_vs_plain": bval / value, "launches_per_step": 4}
+    if world == 1 and args.legs:
+        eng.close()
+        line["batched_mixed"] = batched_mixed(args, local, w.graph, dg, flush)
+        dg.close()
+        line["serve"] = serve_run(args, local)
     if rank == 0 and args.cpu_baseline and ref_available():
-        rr = ReferenceRunner(w)
-        qeq, tot, runs = rr.sample(REF_THREADS, args.ref_budget)
-        for i, (c, over) in enumerate(runs):
-            if not over and c != counts[i]:
-                raise SystemExit(f"reference count {c} differs from ours {counts[i]} (query {i})")
-        line["cpu_baseline"] = {"value": qeq / tot, "unit": "queries/s", "cores": REF_THREADS, "kind": "reference",
-                                "sample": f"{len(runs)} query run(s) from the start of the workload, {tot:.1f} s of "
-                                          f"reference Total time, {qeq:.3f} query-equivalents counted (embeddings "
-                                          f"counted / 1e9 cap), CPU {cpu_info()} ({os.cpu_count()} threads)",
-                                "note": REF_THREADS_NOTE}
+        line["cpu_baseline"] = cpu_baseline(w, counts, min(args.cpu_queries, nq))
     if rank == 0:
         print(json.dumps(line))
     if dist is not None:
@@ -369,10 +436,10 @@ def ours_arm(args, world, rank, local):
 
 # ------------------------------------------------------ other workloads --
 #
-# `--workload batched|join|serve` measure the other rows of the path, each
-# with its own JSON line: the batched path on 2,000 mixed queries, the
-# decomposition + join path against the reference's own join path, and the
-# serving loop at offered loads of 50 / 80 / 95 % of its saturation rate.
+# The batched path on 2,000 mixed queries, the serving loop at offered loads
+# of 50 / 80 / 95 % of its saturation rate (both also keys of the default
+# line at N=1), and the decomposition + join path against the reference's own
+# join path (`--workload join`, its own line).
 
 def _torch_setup(local):
     import torch
@@ -380,14 +447,18 @@ def _torch_setup(local):
     return torch
 
 
-def batched_leg(args, local):
+def batched_mixed(args, local, graph=None, dg=None, flush=None):
+    """2,000 queries of 4-32 vertices (uniform over {4,6,8,12,16,24,32}) on
+    the scale-20 graph: the batched path (one preparation and one
+    enumeration launch for all) against the plain path, counts equal."""
     torch = _torch_setup(local)
     from psm_benchmark_b200 import api, gen
-    w = gen.batched(num_queries=args.queries if args.queries != 200 else 2000, scale=args.scale)
+    w = gen.batched(num_queries=args.mixed_queries, scale=args.scale, graph=graph)
     # candidate buffers of 2,000 queries take about 40 GB
     eng = api.Engine(device=local, arena_bytes=max(args.arena_gb, 64) << 30)
-    dg = api.DataGraph.from_graph(w.graph)
-    flush = torch.empty(256 << 20 >> 2, dtype=torch.float32, device=f"cuda:{local}")
+    own = dg is None
+    dg = dg or api.DataGraph.from_graph(w.graph)
+    flush = flush if flush is not None else torch.empty(256 << 20 >> 2, dtype=torch.float32, device=f"cuda:{local}")
     nq = len(w.queries)
 
     def batched():
@@ -397,16 +468,15 @@ def batched_leg(args, local):
         res = api.match_batch(eng, dg, w.queries, w.method, cap=w.cap, time_limit=args.time_limit)
         return res, time.perf_counter() - t
 
-    for _ in range(args.warmup):
-        batched()
+    steps = args.mixed_steps
+    batched()
     clocks = ClockSampler(local).start()
     dev, wall, res = 0.0, 0.0, None
-    for _ in range(args.steps):
+    for _ in range(steps):
         res, t = batched()
         dev += res[0].prep_ms + res[0].enum_ms
         wall += t
-    clk = clocks.stop()
-    # the plain path on the same queries (one warm pass, one timed pass)
+    # the plain path on the same queries (a warm pass over 50, one timed pass)
     for q in w.queries[:50]:
         api.match(eng, dg, q, w.method, cap=w.cap, time_limit=args.time_limit)
     flush_l2(flush)
@@ -414,30 +484,39 @@ def batched_leg(args, local):
     t = time.perf_counter()
     plain = [api.match(eng, dg, q, w.method, cap=w.cap, time_limit=args.time_limit) for q in w.queries]
     p_wall = time.perf_counter() - t
+    clk = clocks.stop()
     p_dev = sum(r.prep_ms + r.enum_ms for r in plain)
     if [r.count for r in plain] != [r.count for r in res]:
         raise SystemExit("batched counts differ from the plain path")
-    value = nq * args.steps / (dev / 1e3)
+    eng.close()
+    if own:
+        dg.close()
+    value = nq * steps / (dev / 1e3)
     sizes = {}
     for q, r in zip(w.queries, plain):
         sizes.setdefault(q.num_vertices, []).append(r.prep_ms + r.enum_ms)
-    line = {"metric": "queries/sec (batched GPU path, mixed 4-32-vertex queries, CFL_CFL_EXPLORE, cap 1e9)",
-            "value": value, "unit": "queries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dev / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "u32", "data": "synthetic",
+    capped = sum(1 for r in plain if w.cap and r.count >= w.cap)
+    return {"metric": "queries/sec (batched GPU path, mixed 4-32-vertex queries, CFL_CFL_EXPLORE, cap 1e9)",
+            "value": value, "unit": "queries/s", "steps": steps, "ms_per_step": dev / steps,
             "config": {"workload": "batched_rmat_s20", "queries_per_step": nq,
                        "query_sizes": "uniform over {4,6,8,12,16,24,32}", "method": w.method, "cap": w.cap,
                        "l2": "flushed (256 MiB write) before every step"},
-            "embeddings_per_s": sum(r.count for r in res) * args.steps / (dev / 1e3),
-            "e2e": {"value": nq * args.steps / wall, "unit": "queries/s"},
-            "gpu_launches": 4 * args.steps,
+            "embeddings_per_s": sum(r.count for r in res) * steps / (dev / 1e3),
+            "e2e": {"value": nq * steps / wall, "unit": "queries/s"},
+            "gpu_launches_per_step": 4,
             "plain": {"value": nq / (p_dev / 1e3), "e2e": nq / p_wall, "unit": "queries/s",
                       "latency_ms_by_size": {str(k): {"p50": float(np.percentile(v, 50)),
                                                       "p99": float(np.percentile(v, 99))}
                                              for k, v in sorted(sizes.items())}},
             "speedup_vs_plain": value / (nq / (p_dev / 1e3)),
-            "e2e_speedup_vs_plain": (nq * args.steps / wall) / (nq / p_wall),
-            "counts_equal_plain": True, "clocks": clk}
+            "e2e_speedup_vs_plain": (nq * steps / wall) / (nq / p_wall),
+            "counts_equal_plain": True, "capped_queries": capped, "clocks": clk}
+
+
+def batched_leg(args, local):
+    line = batched_mixed(args, local)
+    line.update({"n_gpus": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                 "dtype": "u32", "data": "synthetic", "gpu_launches": 4 * line["steps"]})
     print(json.dumps(line))
 
 
@@ -505,7 +584,7 @@ def join_leg(args, local):
             text = log.read_text()
             tot += float(re.findall(r"Total time \(seconds\): ([0-9.e+-]+)", text)[-1])
             nref += 1
-            if tot > args.ref_budget * 4:
+            if tot > 60:
                 break
         line["cpu_baseline"] = {"value": nref / tot, "unit": "queries/s", "cores": 1, "kind": "reference",
                                 "sample": f"{nref} queries through the reference's join path (-QorCandi Q -Qpattern "
@@ -513,18 +592,23 @@ def join_leg(args, local):
     print(json.dumps(line))
 
 
-def serve_leg(args, local):
+def serve_run(args, local):
+    """Serving on R-MAT scale 24 (edge factor 16, 128 uniform labels): the
+    request stream all at once (saturation), then as Poisson arrivals at 50,
+    80 and 95 % of that rate; latency = completion - scheduled arrival."""
     _torch_setup(local)
     from psm_benchmark_b200 import api, gen
-    nq = args.queries if args.queries != 200 else 5000
+    nq = args.serve_queries
+    scale = args.serve_scale
     t = time.time()
-    w = gen.serve(num_queries=nq, scale=args.scale if args.scale != 20 else 24)
+    w = gen.serve(num_queries=nq, scale=scale)
     dg = api.DataGraph.from_graph(w.graph)
     setup_s = time.time() - t
     lanes = args.lanes
     srv = api.Server(dg, w.method, cap=w.cap, time_limit=args.time_limit, lanes=lanes, max_batch=args.max_batch,
                      lane_arena_bytes=(args.serve_budget_gb << 30) // lanes, full_gpu_lanes=True)
-    # saturation: everything queued at once
+    clocks = ClockSampler(local).start()
+    # warm-up, then saturation: everything queued at once
     for q in w.queries[: min(nq, 500)]:
         srv.submit(q)
     srv.drain(min(nq, 500))
@@ -532,14 +616,17 @@ def serve_leg(args, local):
     for q in w.queries:
         srv.submit(q)
     res = srv.drain(nq, timeout_s=3600)
-    sat = nq / ((max(r.done_ns for r in res) - t0) / 1e9)
+    if len(res) != nq:
+        raise SystemExit(f"serving: {len(res)} of {nq} results")
+    sat_span = (max(r.done_ns for r in res) - t0) / 1e9
+    sat = nq / sat_span
     base = min(r.ticket for r in res)
     counts = {r.ticket - base: r.count for r in res}
+    sat_lat = [(r.done_ns - t0) / 1e6 for r in res]
     loads = {}
-    for load in (0.5, 0.8, 0.95):
+    for load in args.serve_loads:
         rate = load * sat
         arrive = gen.poisson_arrivals(nq, rate, w.seed + int(load * 100))
-        tick0 = None
         start = api.Server.clock_ns()
         sched = {}
         for i, (q, a) in enumerate(zip(w.queries, arrive)):
@@ -547,28 +634,43 @@ def serve_leg(args, local):
             while api.Server.clock_ns() < target:
                 time.sleep(min(0.0005, max(0.0, (target - api.Server.clock_ns()) / 1e9)))
             tk = srv.submit(q)
-            tick0 = tk if tick0 is None else tick0
             sched[tk] = (i, target)
         out = srv.drain(nq, timeout_s=3600)
+        if len(out) != nq:
+            raise SystemExit(f"serving at {load}: {len(out)} of {nq} results")
         lat = [(r.done_ns - sched[r.ticket][1]) / 1e6 for r in out]
         bad = sum(1 for r in out if r.count != counts[sched[r.ticket][0]])
+        if bad:
+            raise SystemExit(f"serving at {load}: {bad} counts differ from the saturation run")
         span = (max(r.done_ns for r in out) - start) / 1e9
-        loads[f"{int(load * 100)}%"] = {"offered_qps": rate, "achieved_qps": nq / span,
-                                        "p50_ms": float(np.percentile(lat, 50)),
-                                        "p99_ms": float(np.percentile(lat, 99)),
-                                        "mean_batch": float(np.mean([r.batch_size for r in out])),
-                                        "count_mismatches_vs_saturation_run": bad}
+        sizes = {}
+        for r, l in zip(out, lat):
+            sizes.setdefault(w.queries[sched[r.ticket][0]].num_vertices, []).append(l)
+        loads[f"{int(round(load * 100))}%"] = {
+            "offered_qps": rate, "achieved_qps": nq / span, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(max(lat)),
+            "p99_ms_by_size": {str(k): float(np.percentile(v, 99)) for k, v in sorted(sizes.items())},
+            "mean_batch": float(np.mean([r.batch_size for r in out])), "counts_equal_saturation_run": True}
+    clk = clocks.stop()
     srv.close()
-    line = {"metric": "queries/sec and p50/p99 latency (serving, continuous batching)", "value": sat,
-            "unit": "queries/s", "n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "serve_rmat", "graph": f"R-MAT scale {args.scale if args.scale != 20 else 24}, "
-                                                          "edge factor 16, 128 uniform labels",
+    dg.close()
+    return {"metric": "queries/sec and p50/p99 latency (serving, continuous batching)", "value": sat,
+            "unit": "queries/s",
+            "config": {"workload": "serve_rmat", "graph": f"R-MAT scale {scale}, edge factor 16, 128 uniform labels",
                        "edges": w.graph.num_edges, "queries": nq,
                        "query_sizes": "{4,8,12,16,24,32} weighted .3/.25/.2/.1/.1/.05", "cap": w.cap,
                        "lanes": lanes, "max_batch": args.max_batch, "budget_gb": args.serve_budget_gb,
                        "setup_s": setup_s},
-            "saturation_qps": sat, "loads": loads}
+            "saturation_qps": sat, "saturation_span_s": sat_span,
+            "saturation_latency_ms": {"p50": float(np.percentile(sat_lat, 50)),
+                                      "p99": float(np.percentile(sat_lat, 99))},
+            "loads": loads, "clocks": clk}
+
+
+def serve_leg(args, local):
+    line = serve_run(args, local)
+    line.update({"n_gpus": 1, "steps": 1, "warmup": 1, "higher_is_better": True, "scaling": "weak",
+                 "vs_baseline": None, "dtype": "u32", "data": "synthetic"})
     print(json.dumps(line))
 
 
@@ -582,11 +684,21 @@ def main():
     ap.add_argument("--scale", type=int, default=20)
     ap.add_argument("--time-limit", type=float, default=600.0)
     ap.add_argument("--arena-gb", type=int, default=8)
-    ap.add_argument("--ref-budget", type=float, default=15.0)
+    ap.add_argument("--ref-limit", type=int, default=600, help="reference time limit per query (s)")
+    ap.add_argument("--ref-mt-limit", type=int, default=10,
+                    help="time limit of the one multi-threaded reference run (s); 0 = skip")
+    ap.add_argument("--cpu-queries", type=int, default=16, help="whole queries in the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-batched", dest="batched", action="store_false")
+    ap.add_argument("--no-legs", dest="legs", action="store_false",
+                    help="leave out the batched_mixed and serve keys of the default line")
     ap.add_argument("--only", default="", help="comma-separated query indices (profiling runs)")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "join", "serve"])
+    ap.add_argument("--mixed-queries", type=int, default=2000)
+    ap.add_argument("--mixed-steps", type=int, default=2)
+    ap.add_argument("--serve-queries", type=int, default=50000)
+    ap.add_argument("--serve-scale", type=int, default=24)
+    ap.add_argument("--serve-loads", type=lambda s: [float(x) for x in s.split(",")], default=[0.5, 0.8, 0.95])
     ap.add_argument("--lanes", type=int, default=4, help="serving lanes")
     ap.add_argument("--max-batch", type=int, default=64, help="serving batch limit")
     ap.add_argument("--serve-budget-gb", type=int, default=120, help="serving device-memory budget")

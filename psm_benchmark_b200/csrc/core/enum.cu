@@ -992,6 +992,12 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
         count = 0;
     }
     count = __shfl_sync(FULL_MASK, count, 0);
+    // Emission keeps q.emit_rows current (one atomic per chunk), so a capped
+    // emitting query stops on it instead of on the lagging published count:
+    // the rows emitted past the cap stay few and fit the caller's buffer.
+    if (lane == 0 && q.emit_buf && q.cap &&
+        *(volatile unsigned long long*)&q.emit_rows >= (unsigned long long)q.cap)
+        cap_reached(q);
     u32 stop = warp_ld_volatile_u32(&q.stop);
     if (!stop && (iter & 255u) == 0 && global_timer_ns() > ctl->deadline_ns) {
         if (lane == 0) {

@@ -69,3 +69,40 @@ def synthetic_cases():
 
 def tables_of(d):
     return {(a, b): (np.array(off, np.uint32), np.array(adj, np.uint32)) for a, b, off, adj in d["tables"]}
+
+
+def digest_cands(cands) -> str:
+    """SHA-256 of candidate sets (a list, by query vertex, of sorted data ids)."""
+    h = hashlib.sha256()
+    for c in cands:
+        c = np.ascontiguousarray(c, np.uint32)
+        h.update(np.uint32(len(c)).tobytes())
+        h.update(c.tobytes())
+    return h.hexdigest()
+
+
+def digest_tables(tables) -> str:
+    """SHA-256 of candidate-edge tables {(a, b): (offsets, entries)}, in (a, b) order."""
+    h = hashlib.sha256()
+    for (a, b) in sorted(tables):
+        off, adj = (np.ascontiguousarray(x, np.uint32) for x in tables[(a, b)])
+        h.update(np.array([a, b, len(off), len(adj)], np.uint32).tobytes())
+        h.update(off.tobytes())
+        h.update(adj.tobytes())
+    return h.hexdigest()
+
+
+@lru_cache(maxsize=1)
+def rmat20():
+    """Pinned queries on the plain benchmark's graph (make_rmat20_golden.py)."""
+    p = GOLDEN / "rmat20_ref.json"
+    return json.loads(p.read_text()) if p.exists() else None
+
+
+def pinned_graph(rec) -> Graph:
+    spec = rec["spec"]
+    g = gen.make_graph("rmat", spec["index"], scale=spec["scale"], edge_factor=spec["edge_factor"],
+                       num_labels=spec["num_labels"])
+    if graph_sha(g) != rec["sha256"]:
+        raise AssertionError(f"generator drift: {rec.get('name', 'rmat20')} graph hash changed")
+    return g

@@ -1,0 +1,166 @@
+"""Parity on the plain benchmark's own graph (R-MAT scale 20, edge factor 8,
+32 uniform labels), against tests/golden/rmat20_ref.json (made by
+tests/golden/make_rmat20_golden.py from the unmodified reference).
+
+Every 12- and 16-vertex query of the benchmark has more than 1e9 embeddings,
+so its count is the cap. The path is pinned here in the ways that survive
+that:
+  * candidates, candidate-edge tables, order and memory cost of the
+    benchmark's own queries equal the reference's (SHA-256 digests);
+  * 4- and 6-vertex queries of the batched workload on the same graph, which
+    the reference finishes, have exactly the reference's counts (plain and
+    batched paths);
+  * every embedding the enumerator counts for a capped benchmark query is a
+    valid, distinct embedding (emission mode, checked on the host), so a
+    capped count cannot hide over-counting;
+  * uncapped counts of benchmark queries agree across both methods (different
+    candidates, tables and orders), with and without the enumerator's caches,
+    and between the plain and batched paths.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from psm_benchmark_b200 import api
+from tests import golden_data as gd
+
+pytestmark = pytest.mark.gpu
+
+METHODS = ("CFL_CFL_EXPLORE", "GQL_GQL_GQL")
+
+
+@pytest.fixture(scope="module")
+def pinned():
+    d = gd.rmat20()
+    if d is None:
+        pytest.fail("tests/golden/rmat20_ref.json is missing")
+    return d
+
+
+@pytest.fixture(scope="module")
+def graph(pinned):
+    return gd.pinned_graph(pinned)
+
+
+@pytest.fixture(scope="module")
+def dev(graph):
+    with api.Engine(arena_bytes=8 << 30) as eng:
+        dg = api.DataGraph.from_graph(graph)
+        yield eng, dg
+        dg.close()
+
+
+def stage_digests(run, q):
+    n = q.num_vertices
+    cands = [run.candidates(u) for u in range(n)]
+    tables = {}
+    for a, b in q.edge_list():
+        for x, y in ((int(a), int(b)), (int(b), int(a))):
+            tables[(x, y)] = run.table(x, y)
+    o, p = run.order()
+    return {"cands_sha": gd.digest_cands(cands), "cand_counts": [len(c) for c in cands],
+            "tables_sha": gd.digest_tables(tables), "order": [int(x) for x in o], "pivot": [int(x) for x in p],
+            "memory": run.result.memory_bytes}
+
+
+def check_stages(run, q, ref):
+    got = stage_digests(run, q)
+    assert got["cand_counts"] == ref["cand_counts"]
+    assert got["cands_sha"] == ref["cands_sha"]
+    assert got["tables_sha"] == ref["tables_sha"]
+    assert got["memory"] == ref["memory"]
+    assert got["order"] == ref["order"]
+    assert got["pivot"][1:] == ref["pivot"][1:]
+
+
+def test_benchmark_queries_stages_match_reference(pinned, dev):
+    eng, dg = dev
+    assert len(pinned["bench"]) >= 40
+    for e in pinned["bench"]:
+        q = gd.query_from_rec(e["query"])
+        for m in METHODS:
+            with api.Run(eng, dg, q, m, cap=pinned["cap"], time_limit=60) as run:
+                check_stages(run, q, e["methods"][m])
+                assert run.result.count == pinned["cap"]
+
+
+def test_small_queries_counts_match_reference(pinned, dev):
+    eng, dg = dev
+    small = pinned["small"]
+    assert len(small) >= 40
+    for m in METHODS:
+        qs = [gd.query_from_rec(e["query"]) for e in small]
+        want = [e["methods"][m]["count"] for e in small]
+        for q, e, c in zip(qs, small, want):
+            with api.Run(eng, dg, q, m, cap=pinned["cap"], time_limit=60) as run:
+                assert run.result.count == c, (e["index"], m)
+                assert run.result.count_internal == c
+                check_stages(run, q, e["methods"][m])
+        batch = api.match_batch(eng, dg, qs, m, cap=pinned["cap"], time_limit=60)
+        assert [r.count for r in batch] == want
+
+
+def valid_distinct(g, q, emb):
+    """Every row an embedding of q in g: labels equal, injective, every query
+    edge on a data edge; rows pairwise distinct."""
+    assert (g.labels[emb] == q.labels[None, :]).all()
+    srt = np.sort(emb, axis=1)
+    assert (srt[:, 1:] != srt[:, :-1]).all()
+    keys = g.edge_list()
+    keys = np.sort(keys[:, 0] * g.num_vertices + keys[:, 1])
+    for a, b in q.edge_list():
+        lo = np.minimum(emb[:, a], emb[:, b]).astype(np.int64)
+        hi = np.maximum(emb[:, a], emb[:, b]).astype(np.int64)
+        k = lo * g.num_vertices + hi
+        pos = np.searchsorted(keys, k)
+        assert (pos < len(keys)).all() and (keys[np.minimum(pos, len(keys) - 1)] == k).all()
+    rows = np.ascontiguousarray(emb).view(np.dtype((np.void, emb.dtype.itemsize * emb.shape[1])))
+    assert len(np.unique(rows)) == len(emb)
+
+
+def test_capped_counts_are_distinct_valid_embeddings(pinned, graph, dev):
+    eng, dg = dev
+    cap = 1 << 16
+    room = 1 << 23
+    for e in pinned["bench"][::3]:
+        q = gd.query_from_rec(e["query"])
+        with api.Run(eng, dg, q, "CFL_CFL_EXPLORE", cap=cap, time_limit=60, emit=room) as run:
+            emb = run.embeddings()
+            assert run.result.count == cap
+            # every counted embedding was emitted: the buffer did not fill up
+            # and holds as many rows as the enumerator counted
+            assert len(emb) < room
+            assert len(emb) == run.result.count_internal >= cap
+            valid_distinct(graph, q, emb)
+
+
+def test_uncapped_counts_agree_across_paths(pinned, dev):
+    """Without the cap the benchmark queries' counts exceed it. Where the
+    device finishes them in a few seconds, the count is the same under both
+    methods, without the enumerator's caches, and through the batched path."""
+    eng, dg = dev
+    os.environ["PSM_ENUM_CACHE"] = "0"
+    try:
+        plain_eng = api.Engine(arena_bytes=8 << 30)
+    finally:
+        del os.environ["PSM_ENUM_CACHE"]
+    agreed = 0
+    try:
+        for e in pinned["bench"]:
+            q = gd.query_from_rec(e["query"])
+            first = api.match(eng, dg, q, "CFL_CFL_EXPLORE", cap=0, time_limit=1.0)
+            if first.overtime:
+                continue
+            assert first.count > pinned["cap"]
+            for m, en in (("GQL_GQL_GQL", eng), ("CFL_CFL_EXPLORE", plain_eng)):
+                r = api.match(en, dg, q, m, cap=0, time_limit=30.0)
+                assert not r.overtime and r.count == first.count, (e["index"], m)
+            b = api.match_batch(eng, dg, [q, q], "CFL_CFL_EXPLORE", cap=0, time_limit=30.0)
+            assert [r.count for r in b] == [first.count] * 2
+            agreed += 1
+            if agreed == 8:
+                break
+    finally:
+        plain_eng.close()
+    assert agreed >= 4

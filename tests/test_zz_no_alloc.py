@@ -91,8 +91,14 @@ def _kept_failed_run(dg, q):
 def test_recount_noalloc_refuses_failed_preparation():
     g = gd.synthetic_graph("rmat12")
     case = dict(gd.synthetic_cases())["rmat12"]
-    q = gd.query_from_rec(case["queries"][0]["query"])
+    queries = [gd.query_from_rec(e["query"]) for e in case["queries"]]
     dg = api.DataGraph.from_graph(g)
+    # the query with the largest candidate tables leaves the widest window of
+    # arena sizes where the host-side setup fits but the tables do not
+    with api.Engine(arena_bytes=1 << 30) as big:
+        sizes = [api.match(big, dg, q, "CFL_CFL_EXPLORE", cap=1).table_entries for q in queries]
+    q = queries[max(range(len(queries)), key=sizes.__getitem__)]
+    assert max(sizes) * 4 > 1 << 16
     eng, h = _kept_failed_run(dg, q)
     try:
         cnt = C.c_uint64(7)
