@@ -653,6 +653,25 @@ def serve_run(args, local):
             "mean_batch": float(np.mean([r.batch_size for r in out])), "counts_equal_saturation_run": True}
     clk = clocks.stop()
     srv.close()
+    # the plain path (one query per launch sequence, whole GPU) on the first
+    # requests of the same stream, for the served / plain ratio
+    plain = None
+    if args.serve_plain > 0:
+        eng = api.Engine(device=local, arena_bytes=args.arena_gb << 30)
+        sample = w.queries[: min(nq, args.serve_plain)]
+        for q in sample[:20]:
+            api.match(eng, dg, q, w.method, cap=w.cap, time_limit=args.time_limit)
+        t = time.perf_counter()
+        pres = [api.match(eng, dg, q, w.method, cap=w.cap, time_limit=args.time_limit) for q in sample]
+        p_wall = time.perf_counter() - t
+        eng.close()
+        p_dev = sum(r.prep_ms + r.enum_ms for r in pres) / 1e3
+        bad = sum(1 for i, r in enumerate(pres) if r.count != counts[i])
+        if bad:
+            raise SystemExit(f"serving: {bad} counts differ from the plain path")
+        plain = {"queries": len(sample), "value": len(sample) / p_dev, "e2e": len(sample) / p_wall,
+                 "unit": "queries/s", "served_saturation_vs_plain_e2e": sat / (len(sample) / p_wall),
+                 "counts_equal_served": True}
     dg.close()
     return {"metric": "queries/sec and p50/p99 latency (serving, continuous batching)", "value": sat,
             "unit": "queries/s",
@@ -664,7 +683,7 @@ def serve_run(args, local):
             "saturation_qps": sat, "saturation_span_s": sat_span,
             "saturation_latency_ms": {"p50": float(np.percentile(sat_lat, 50)),
                                       "p99": float(np.percentile(sat_lat, 99))},
-            "loads": loads, "clocks": clk}
+            "loads": loads, "plain": plain, "clocks": clk}
 
 
 def serve_leg(args, local):
@@ -698,6 +717,8 @@ def main():
     ap.add_argument("--mixed-steps", type=int, default=2)
     ap.add_argument("--serve-queries", type=int, default=50000)
     ap.add_argument("--serve-scale", type=int, default=24)
+    ap.add_argument("--serve-plain", type=int, default=2000,
+                    help="requests of the stream also run through the plain path (served / plain ratio)")
     ap.add_argument("--serve-loads", type=lambda s: [float(x) for x in s.split(",")], default=[0.5, 0.8, 0.95])
     ap.add_argument("--lanes", type=int, default=4, help="serving lanes")
     ap.add_argument("--max-batch", type=int, default=64, help="serving batch limit")

@@ -10,9 +10,11 @@ the rest of the suite; it also passes when run alone.
 """
 import ctypes as C
 
+import numpy as np
 import pytest
 
-from psm_benchmark_b200 import api
+from psm_benchmark_b200 import api, gen
+from psm_benchmark_b200.graphs import Graph
 from psm_benchmark_b200 import native as N
 from tests import golden_data as gd
 
@@ -61,7 +63,8 @@ def _kept_failed_run(dg, q):
     bisecting the context's arena size between a size where the host-side
     setup already fails and one where the query runs."""
     qb = api._QueryBuf(q)
-    opt = api.options("CFL_CFL_EXPLORE", 0, 60.0, 0)
+    # cap 1: a query that prepares successfully stops at its first embedding
+    opt = api.options("CFL_CFL_EXPLORE", 1, 60.0, 0)
     lo, hi = 1 << 20, 1 << 30
     for _ in range(40):
         size = (lo + hi) // 2
@@ -89,16 +92,15 @@ def _kept_failed_run(dg, q):
 
 
 def test_recount_noalloc_refuses_failed_preparation():
-    g = gd.synthetic_graph("rmat12")
-    case = dict(gd.synthetic_cases())["rmat12"]
-    queries = [gd.query_from_rec(e["query"]) for e in case["queries"]]
+    # a star of six same-label leaves on a single-label graph: its candidate
+    # tables (every candidate's whole row, per query edge and direction) are
+    # large, which leaves a wide window of arena sizes where the host-side
+    # setup fits but the tables do not
+    g = gen.make_graph("rmat", 40, scale=11, edge_factor=8, num_labels=1)
+    q = Graph.from_edges(7, np.zeros(7, np.uint32), [(0, i) for i in range(1, 7)])
     dg = api.DataGraph.from_graph(g)
-    # the query with the largest candidate tables leaves the widest window of
-    # arena sizes where the host-side setup fits but the tables do not
     with api.Engine(arena_bytes=1 << 30) as big:
-        sizes = [api.match(big, dg, q, "CFL_CFL_EXPLORE", cap=1).table_entries for q in queries]
-    q = queries[max(range(len(queries)), key=sizes.__getitem__)]
-    assert max(sizes) * 4 > 1 << 16
+        assert api.match(big, dg, q, "CFL_CFL_EXPLORE", cap=1).table_entries * 4 > 1 << 20
     eng, h = _kept_failed_run(dg, q)
     try:
         cnt = C.c_uint64(7)
