@@ -623,6 +623,17 @@ def serve_run(args, local):
     base = min(r.ticket for r in res)
     counts = {r.ticket - base: r.count for r in res}
     sat_lat = [(r.done_ns - t0) / 1e6 for r in res]
+    # batches of the saturation run: (lane, start) -> size, prep / enum ms
+    batches = {}
+    for r in res:
+        batches[(r.lane, r.start_ns)] = (r.batch_size, r.prep_ms, r.enum_ms)
+    lane_busy = {}
+    for (ln, _), (_, pm, em) in batches.items():
+        lane_busy[ln] = lane_busy.get(ln, 0.0) + pm + em
+    batch_stats = {"batches": len(batches), "mean_batch": float(np.mean([b[0] for b in batches.values()])),
+                   "prep_ms_total": float(sum(b[1] for b in batches.values())),
+                   "enum_ms_total": float(sum(b[2] for b in batches.values())),
+                   "lane_device_busy_frac": {str(k): v / 1e3 / sat_span for k, v in sorted(lane_busy.items())}}
     loads = {}
     for load in args.serve_loads:
         rate = load * sat
@@ -683,6 +694,7 @@ def serve_run(args, local):
             "saturation_qps": sat, "saturation_span_s": sat_span,
             "saturation_latency_ms": {"p50": float(np.percentile(sat_lat, 50)),
                                       "p99": float(np.percentile(sat_lat, 99))},
+            "saturation_batches": batch_stats,
             "loads": loads, "plain": plain, "clocks": clk}
 
 

@@ -195,6 +195,44 @@ typedef struct psm_join_result {
  * counted, not materialised. opt->cap applies to the final count. */
 int psm_match_join(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
                    uint32_t max_unit_vertices, psm_join_result* res);
+/* Decomposition patterns of the join path: the reference's -Qpattern values
+ * (matching/StudyPerformance.cpp:429-437, utility/splitGraph/SplitGraph.cpp:
+ * split_star :895, split_twintwig :875 with optimalDecomposition :671-872,
+ * split_seed :913, split_hybrid_rnd :38-108) and two of this library's own
+ * that bound the unit size. */
+typedef enum psm_split_pattern {
+    PSM_SPLIT_BOUNDED = 0,    /* connected units of at most max_unit vertices (psm_match_join) */
+    PSM_SPLIT_STAR = 1,       /* stars around a vertex cover (max_unit > 1 splits larger stars) */
+    PSM_SPLIT_TWINTWIG = 2,   /* units of one or two edges sharing a vertex, chosen by the card() cost model */
+    PSM_SPLIT_SEED = 3,       /* twin-twigs, triangles where the query closes them */
+    PSM_SPLIT_SKETCHTREE = 4, /* root-to-leaf paths of a depth-first tree, joined along the tree */
+    PSM_SPLIT_COST = 5        /* bounded units and join tree of least estimated materialised rows */
+} psm_split_pattern;
+/* Join paradigms (the reference's -JoinMethod LEFTDEEP / BUSHY,
+ * StudyPerformance.cpp:421-426); SKETCHTREE always joins along its tree
+ * (JoinCollect::recur_collect, matching/JoinCollect.cpp:156-235). */
+typedef enum psm_join_method { PSM_JOIN_LEFTDEEP = 0, PSM_JOIN_BUSHY = 1 } psm_join_method;
+typedef struct psm_join_options {
+    uint32_t pattern;      /* psm_split_pattern */
+    uint32_t join_method;  /* psm_join_method */
+    uint32_t max_unit;     /* unit bound of BOUNDED / COST (required) and STAR (0 = none) */
+    uint32_t reserved;
+} psm_join_options;
+/* psm_match_join with a chosen decomposition pattern and join paradigm
+ * (replaces split_Q_test's SplitGraph + sequence_collect / recur_collect).
+ * res->join_rows[j] = rows out of the j-th join executed (join_rows[0] =
+ * the first unit evaluated); the last join is counted, not materialised. */
+int psm_match_join_ex(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
+                      const psm_join_options* jo, psm_join_result* res);
+/* The decomposition and join plan psm_match_join_ex would use, on the host
+ * (COST and the twin-twig searches then use the reference's label-blind
+ * card model with data_vertices / data_edges): unit_masks[PSM_MAX_UNITS];
+ * the plan as binary joins in execution order, join_ops[2 * j] and
+ * join_ops[2 * j + 1] naming the operands of join j (a unit k < num_units,
+ * or num_units + i = the result of join i). */
+int psm_query_decompose_ex(const psm_query_desc* q, const psm_join_options* jo, double data_vertices,
+                           double data_edges, uint32_t* num_units, uint32_t* unit_masks, uint32_t* num_joins,
+                           uint32_t* join_ops);
 /* The decomposition psm_match_join uses (host only): *num_units units,
  * unit_masks[PSM_MAX_UNITS] their vertex sets. */
 int psm_query_decompose(const psm_query_desc* q, uint32_t max_unit_vertices, uint32_t* num_units,

@@ -238,16 +238,19 @@ class JoinResult:
 
 
 def match_join(engine: Engine, data: DataGraph, query: Graph, method: str = "CFL_CFL_EXPLORE",
-               max_unit_vertices: int = 12, cap: int = 0, time_limit: float = 60.0) -> JoinResult:
+               max_unit_vertices: int = 12, cap: int = 0, time_limit: float = 60.0, pattern: str = "BOUNDED",
+               join_method: str = "LEFTDEEP") -> JoinResult:
     """Decomposition + hash-join path: the query is filtered and tabled
-    whole, split into connected units of at most max_unit_vertices vertices,
-    each unit's embeddings are materialised on the device and joined
-    left-deep on shared query vertices."""
+    whole, split into units (pattern: BOUNDED = connected units of at most
+    max_unit_vertices vertices; the reference's STAR, TWINTWIG, SEED,
+    SKETCHTREE; COST = bounded units of least estimated cost), each unit's
+    embeddings are materialised on the device and joined on shared query
+    vertices, left-deep or bushy."""
     qb = _QueryBuf(query)
     opt = options(method, cap, time_limit)
+    jo = N.JoinOptions(N.SPLIT_PATTERNS[pattern], N.JOIN_METHODS[join_method], int(max_unit_vertices), 0)
     r = N.JoinResult()
-    N.check(N.lib().psm_match_join(engine._h, data._h, C.byref(qb.desc), C.byref(opt), int(max_unit_vertices),
-                                   C.byref(r)))
+    N.check(N.lib().psm_match_join_ex(engine._h, data._h, C.byref(qb.desc), C.byref(opt), C.byref(jo), C.byref(r)))
     u = r.units
     return JoinResult(count=r.count, units=list(r.unit_mask[:u]), unit_rows=list(r.unit_rows[:u]),
                       join_rows=list(r.join_rows[:u]), prep_ms=r.prep_ms, enum_ms=r.enum_ms, join_ms=r.join_ms,
@@ -261,6 +264,22 @@ def decompose(query: Graph, max_unit_vertices: int = 12) -> list:
     masks = (C.c_uint32 * N.MAX_UNITS)()
     N.check(N.lib().psm_query_decompose(C.byref(qb.desc), int(max_unit_vertices), C.byref(n), masks))
     return list(masks[: n.value])
+
+
+def join_plan(query: Graph, pattern: str = "BOUNDED", join_method: str = "LEFTDEEP", max_unit_vertices: int = 12,
+              data_vertices: float = 1e6, data_edges: float = 8e6):
+    """The units and binary joins psm_match_join_ex would use (host only; the
+    cost searches use the label-blind card model of a data graph with the
+    given sizes). Returns (unit masks, [(left, right), ...]): operands are
+    unit indices, or len(units) + i for the result of join i."""
+    qb = _QueryBuf(query)
+    jo = N.JoinOptions(N.SPLIT_PATTERNS[pattern], N.JOIN_METHODS[join_method], int(max_unit_vertices), 0)
+    n, nj = C.c_uint32(), C.c_uint32()
+    masks = (C.c_uint32 * N.MAX_UNITS)()
+    ops = (C.c_uint32 * (4 * N.MAX_UNITS))()
+    N.check(N.lib().psm_query_decompose_ex(C.byref(qb.desc), C.byref(jo), float(data_vertices), float(data_edges),
+                                           C.byref(n), masks, C.byref(nj), ops))
+    return list(masks[: n.value]), [(ops[2 * j], ops[2 * j + 1]) for j in range(nj.value)]
 
 
 def hash_join(engine: Engine, r_rows: np.ndarray, r_vertex, s_rows: np.ndarray, s_vertex, vertex_label=None,

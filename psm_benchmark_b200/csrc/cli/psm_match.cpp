@@ -8,9 +8,11 @@
 // entry of -threadnums and every FILTER_ORDER_ENGINE triple of -BackMethods,
 // one query run and one log block. Q mode (-QorCandi Q, split_Q_test,
 // StudyPerformance.cpp:100-1037) runs the decomposition + hash-join path
-// (psm_match_join): units of at most -max_unit vertices (default 12) replace
-// the reference's -Qpattern decompositions, whose name is recorded; the
-// count does not depend on the decomposition.
+// (psm_match_join_ex) with the -Qpattern decomposition (STAR, the default,
+// TWINTWIG, SEED, SKETCHTREE; also this library's BOUNDED and COST, whose
+// units have at most -max_unit vertices, default 12) and the -JoinMethod
+// paradigm (LEFTDEEP, the default, or BUSHY); -max_unit also splits STAR's
+// stars. The count does not depend on the decomposition.
 //
 // Differences a caller can see:
 //  - every engine name is accepted and served by the set-intersection
@@ -46,6 +48,10 @@ struct Flags {
     std::string get(const std::string& k, const std::string& def) const {
         auto it = kv.find(k);
         return it == kv.end() || it->second.empty() ? def : it->second;
+    }
+    bool has(const std::string& k) const {
+        auto it = kv.find(k);
+        return it != kv.end() && !it->second.empty();
     }
 };
 
@@ -181,7 +187,28 @@ int main(int argc, char** argv) {
     const std::vector<std::string> methods = split(f.get("-BackMethods", "DPiso"), ',');
     const int device = std::atoi(f.get("-device", "0").c_str());
     const double arena_gb = std::atof(f.get("-arena_gb", "16").c_str());
+    const bool have_max_unit = f.has("-max_unit");
     const uint32_t max_unit = (uint32_t)std::atoi(f.get("-max_unit", "12").c_str());
+    const std::string qpattern = f.get("-Qpattern", "STAR"), join_method = f.get("-JoinMethod", "LEFTDEEP");
+    psm_join_options jo{PSM_SPLIT_STAR, PSM_JOIN_LEFTDEEP, have_max_unit ? max_unit : 0u, 0};
+    if (mode == "Q") {
+        if (qpattern == "STAR") jo.pattern = PSM_SPLIT_STAR;
+        else if (qpattern == "TWINTWIG") jo.pattern = PSM_SPLIT_TWINTWIG;
+        else if (qpattern == "SEED") jo.pattern = PSM_SPLIT_SEED;
+        else if (qpattern == "SKETCHTREE") jo.pattern = PSM_SPLIT_SKETCHTREE;
+        else if (qpattern == "BOUNDED") jo.pattern = PSM_SPLIT_BOUNDED, jo.max_unit = max_unit;
+        else if (qpattern == "COST") jo.pattern = PSM_SPLIT_COST, jo.max_unit = max_unit;
+        else {
+            log << "Error: The split pattern '" << qpattern << "' is not defined."; log.end();
+            return 1;
+        }
+        if (join_method == "LEFTDEEP") jo.join_method = PSM_JOIN_LEFTDEEP;
+        else if (join_method == "BUSHY") jo.join_method = PSM_JOIN_BUSHY;
+        else {
+            log << "Error: The join method '" << join_method << "' is not defined."; log.end();
+            return 1;
+        }
+    }
 
     auto t0 = std::chrono::steady_clock::now();
     psm_graph* g = nullptr;
@@ -225,8 +252,8 @@ int main(int argc, char** argv) {
                 log << "Split Type: " << split_type; log.end();
                 log << "Schedule Type: " << schedule; log.end();
             } else {
-                log << "QuerySplit Pattern: " << f.get("-Qpattern", "STAR"); log.end();
-                log << "Join Paradigm: " << f.get("-JoinMethod", "LEFTDEEP"); log.end();
+                log << "QuerySplit Pattern: " << qpattern; log.end();
+                log << "Join Paradigm: " << join_method; log.end();
             }
             log << "Filter Type: " << ft; log.end();
             log << "Order Type: " << ot; log.end();
@@ -258,7 +285,7 @@ int main(int argc, char** argv) {
             psm_result r{};
             psm_join_result jr{};
             auto w0 = std::chrono::steady_clock::now();
-            int rc = mode == "C" ? psm_match(ctx, g, &q, &opt, &r) : psm_match_join(ctx, g, &q, &opt, max_unit, &jr);
+            int rc = mode == "C" ? psm_match(ctx, g, &q, &opt, &r) : psm_match_join_ex(ctx, g, &q, &opt, &jo, &jr);
             auto w1 = std::chrono::steady_clock::now();
             if (rc != PSM_OK && rc != PSM_ERR_TIMEOUT) {
                 std::cerr << "psm_match: " << psm_status_string(rc) << ": " << psm_last_error() << "\n";

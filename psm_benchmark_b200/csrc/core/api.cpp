@@ -793,6 +793,21 @@ int query_adjacency(const psm_query_desc& q, u32* adj) {
     return PSM_OK;
 }
 
+// The plan as binary joins in execution order (operands: unit k, or
+// nunits + i = the result of join i); returns the operand id of `node`.
+u32 plan_ops(const Decomposition& d, u32 node, std::vector<u32>& ops) {
+    const JoinNode& nd = d.nodes[node];
+    if (nd.unit >= 0) return (u32)nd.unit;
+    u32 acc = plan_ops(d, nd.child[0], ops);
+    for (u32 i = 1; i < nd.nchild; ++i) {
+        const u32 r = plan_ops(d, nd.child[i], ops);
+        ops.push_back(acc);
+        ops.push_back(r);
+        acc = d.nunits + (u32)(ops.size() / 2 - 1);
+    }
+    return acc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -811,9 +826,40 @@ int psm_query_decompose(const psm_query_desc* q, uint32_t max_unit_vertices, uin
     return PSM_OK;
 }
 
+
+int psm_query_decompose_ex(const psm_query_desc* q, const psm_join_options* jo, double data_vertices,
+                           double data_edges, uint32_t* num_units, uint32_t* unit_masks, uint32_t* num_joins,
+                           uint32_t* join_ops) {
+    if (!q || !jo || !num_units || !unit_masks) return fail(PSM_ERR_ARG, "null argument");
+    u32 adj[PSM_MAXQ], cnt[PSM_MAXQ] = {};
+    int rc = query_adjacency(*q, adj);
+    if (rc) return rc;
+    PlanStats st;
+    st.data_vertices = data_vertices;
+    st.data_edges = data_edges;
+    Decomposition dec;
+    std::string err;
+    if (psm_decompose_pattern(q->num_vertices, adj, cnt, jo->pattern, jo->join_method, jo->max_unit, st, &dec, &err))
+        return fail(PSM_ERR_ARG, err);
+    *num_units = dec.nunits;
+    for (u32 k = 0; k < dec.nunits; ++k) unit_masks[k] = dec.units[k].mask;
+    std::vector<u32> ops;
+    plan_ops(dec, dec.root, ops);
+    if (num_joins) *num_joins = (u32)(ops.size() / 2);
+    if (join_ops)
+        for (u32 i = 0; i < ops.size(); ++i) join_ops[i] = ops[i];
+    return PSM_OK;
+}
+
 int psm_match_join(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
                    uint32_t max_unit_vertices, psm_join_result* res) {
-    if (!ctx || !g || !q || !opt || !res) return fail(PSM_ERR_ARG, "null argument");
+    const psm_join_options jo{PSM_SPLIT_BOUNDED, PSM_JOIN_LEFTDEEP, max_unit_vertices, 0};
+    return psm_match_join_ex(ctx, g, q, opt, &jo, res);
+}
+
+int psm_match_join_ex(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,
+                      const psm_join_options* jo, psm_join_result* res) {
+    if (!ctx || !g || !q || !opt || !res || !jo) return fail(PSM_ERR_ARG, "null argument");
     memset(res, 0, sizeof(*res));
     if (opt->emit) return fail(PSM_ERR_ARG, "the join path counts; emit is not supported");
     u32 adj[PSM_MAXQ];
@@ -836,10 +882,32 @@ int psm_match_join(psm_context* ctx, const psm_graph* g, const psm_query_desc* q
     res->prep_ms = pr.prep_ms;
     res->memory_bytes = pr.memory_bytes;
     const QState& hq = run.hq;
-    // 2. units
+    const u32 n = q->num_vertices;
+    // 2. units and join plan; the cost-based pattern reads the candidate
+    // counts and the table sizes (fraction of candidate pairs that are data
+    // edges) of the prepared query
+    PlanStats st;
+    st.data_vertices = g->V;
+    st.data_edges = (double)g->nnz / 2;
+    std::vector<double> cand(n), edge_p((size_t)n * n, 0.0);
+    if (jo->pattern == PSM_SPLIT_COST && !hq.empty) {
+        const QDesc& d = *run.hdesc;
+        for (u32 u = 0; u < n; ++u) cand[u] = hq.cnt[u];
+        for (u32 e = 0; e < d.e_first[n]; ++e) {
+            const u32 a = d.e_src[e], b = d.e_dst[e];
+            u32 ends[2] = {0, 0};
+            CK(cudaMemcpy(&ends[0], hq.P + hq.e_row_base[e], sizeof(u32), cudaMemcpyDeviceToHost));
+            CK(cudaMemcpy(&ends[1], hq.P + hq.e_row_base[e] + hq.cnt[a], sizeof(u32), cudaMemcpyDeviceToHost));
+            const double pairs = (double)hq.cnt[a] * hq.cnt[b];
+            edge_p[(size_t)a * n + b] = pairs > 0 ? (ends[1] - ends[0]) / pairs : 0.0;
+        }
+        st.cand = cand.data();
+        st.edge_p = edge_p.data();
+    }
     Decomposition dec;
     std::string err;
-    if (psm_decompose(q->num_vertices, adj, hq.cnt, max_unit_vertices, &dec, &err)) return fail(PSM_ERR_ARG, err);
+    if (psm_decompose_pattern(n, adj, hq.cnt, jo->pattern, jo->join_method, jo->max_unit, st, &dec, &err))
+        return fail(PSM_ERR_ARG, err);
     const u32 U = dec.nunits;
     res->units = U;
     for (u32 k = 0; k < U; ++k) res->unit_mask[k] = dec.units[k].mask;
@@ -893,9 +961,7 @@ int psm_match_join(psm_context* ctx, const psm_graph* g, const psm_query_desc* q
     rc = run_units(0);
     if (rc) return rc;
     u64 used = 0;
-    for (u32 k = 0; k < U; ++k) {
-        res->unit_rows[k] = dr[k].count;
-    }
+    for (u32 k = 0; k < U; ++k) res->unit_rows[k] = dr[k].count;
     if (U == 1) {
         CK(cudaEventRecord(ctx->ev[1], ctx->st));
         CK(cudaEventSynchronize(ctx->ev[1]));
@@ -922,33 +988,32 @@ int psm_match_join(psm_context* ctx, const psm_graph* g, const psm_query_desc* q
     for (u32 k = 0; k < U; ++k)
         if (dr[k].emit_rows != caps[k]) return fail(PSM_ERR_INTERNAL, "unit emission differs from its count");
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    // 4. left-deep joins in unit order; the last one is counted
+    // 4. the joins of the plan, in execution order; the last one is counted
     const u32* label = run.hdesc->label;
-    Rel acc;
-    acc.rows = bufs[0];
-    acc.n = caps[0];
-    acc.ncols = dec.units[0].n;
-    for (u32 i = 0; i < acc.ncols; ++i) acc.vert[i] = dec.units[0].order[i];
-    res->join_rows[0] = acc.n;
-    u64 total = acc.n;
-    for (u32 k = 1; k < U; ++k) {
-        Rel unit;
-        unit.rows = bufs[k];
-        unit.n = caps[k];
-        unit.ncols = dec.units[k].n;
-        for (u32 i = 0; i < unit.ncols; ++i) unit.vert[i] = dec.units[k].order[i];
-        const bool last = k + 1 == U;
+    std::vector<u32> ops;
+    plan_ops(dec, dec.root, ops);
+    const u32 J = (u32)(ops.size() / 2);
+    std::vector<Rel> results(J);
+    auto operand = [&](u32 id) -> Rel {
+        if (id >= U) return results[id - U];
+        Rel r;
+        r.rows = bufs[id];
+        r.n = caps[id];
+        r.ncols = dec.units[id].n;
+        for (u32 i = 0; i < r.ncols; ++i) r.vert[i] = dec.units[id].order[i];
+        return r;
+    };
+    res->join_rows[0] = caps[ops[0]];
+    u64 total = 0;
+    for (u32 j = 0; j < J; ++j) {
+        const Rel a = operand(ops[2 * j]), b = operand(ops[2 * j + 1]);
+        const bool last = j + 1 == J;
         // build on the smaller side
-        const bool build_acc = acc.n <= unit.n;
-        Rel next;
-        rc = join_rels(ctx, ar, label, build_acc ? acc : unit, build_acc ? unit : acc, last, &next, &total, &used);
+        const bool build_a = a.n <= b.n;
+        rc = join_rels(ctx, ar, label, build_a ? a : b, build_a ? b : a, last, &results[j], &total, &used);
         if (rc) return rc;
-        res->join_rows[k] = total;
-        if (!last) acc = next;
-        if (total == 0) {
-            for (u32 j = k + 1; j < U; ++j) res->join_rows[j] = 0;
-            break;
-        }
+        if (j + 1 < PSM_MAX_UNITS) res->join_rows[j + 1] = total;
+        if (total == 0) break;  // an empty partial result empties the query
     }
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     CK(cudaEventSynchronize(ctx->ev[2]));

@@ -25,7 +25,7 @@ EXPORTS = [
     "psm_context_create", "psm_context_free",
     "psm_match", "psm_run_create", "psm_run_candidates", "psm_run_table", "psm_run_order",
     "psm_run_embeddings", "psm_run_free", "psm_match_batch", "psm_run_recount_noalloc",
-    "psm_match_join", "psm_query_decompose", "psm_hash_join",
+    "psm_match_join", "psm_query_decompose", "psm_hash_join", "psm_match_join_ex", "psm_query_decompose_ex",
     "psm_server_create", "psm_server_submit", "psm_server_poll", "psm_server_pending", "psm_server_estimate",
     "psm_server_clock_ns", "psm_server_destroy",
     "psm_graph_load_binary", "psm_graph_store_binary", "psm_graph_convert", "psm_graph_convert_edgelist",
@@ -72,6 +72,15 @@ class RequestResult(C.Structure):
                 ("batch_size", C.c_uint32), ("lane", C.c_uint32), ("prep_ms", C.c_double), ("enum_ms", C.c_double)]
 
 
+SPLIT_PATTERNS = {"BOUNDED": 0, "STAR": 1, "TWINTWIG": 2, "SEED": 3, "SKETCHTREE": 4, "COST": 5}
+JOIN_METHODS = {"LEFTDEEP": 0, "BUSHY": 1}
+
+
+class JoinOptions(C.Structure):
+    _fields_ = [("pattern", C.c_uint32), ("join_method", C.c_uint32), ("max_unit", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
 class JoinResult(C.Structure):
     _fields_ = [("count", C.c_uint64), ("units", C.c_uint32), ("status", C.c_uint32),
                 ("unit_mask", C.c_uint32 * MAX_UNITS), ("unit_rows", C.c_uint64 * MAX_UNITS),
@@ -114,6 +123,10 @@ def lib():
         "psm_match_join": ([vp, vp, C.POINTER(QueryDesc), C.POINTER(Options), C.c_uint32, C.POINTER(JoinResult)],
                            C.c_int),
         "psm_query_decompose": ([C.POINTER(QueryDesc), C.c_uint32, u32p, u32p], C.c_int),
+        "psm_match_join_ex": ([vp, vp, C.POINTER(QueryDesc), C.POINTER(Options), C.POINTER(JoinOptions),
+                               C.POINTER(JoinResult)], C.c_int),
+        "psm_query_decompose_ex": ([C.POINTER(QueryDesc), C.POINTER(JoinOptions), C.c_double, C.c_double, u32p, u32p,
+                                    u32p, u32p], C.c_int),
         "psm_server_create": ([C.c_int, vp, C.POINTER(Options), C.POINTER(ServerConfig), C.POINTER(vp)], C.c_int),
         "psm_server_submit": ([vp, C.POINTER(QueryDesc), C.POINTER(C.c_uint64)], C.c_int),
         "psm_server_poll": ([vp, C.POINTER(RequestResult), C.c_uint32, u32p, C.c_double], C.c_int),

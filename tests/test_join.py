@@ -154,3 +154,42 @@ def test_join_single_unit_and_empty(engine):
     q2 = type(q).from_edges(q.num_vertices, lab, q.edge_list())
     r = api.match_join(engine, dg, q2, "CFL_CFL_EXPLORE", max_unit_vertices=4)
     assert r.count == 0
+
+
+PATTERNS = ["STAR", "TWINTWIG", "SEED", "SKETCHTREE"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pattern", PATTERNS + ["COST"])
+def test_join_patterns_match_reference_counts(engine, pattern):  # noqa: F811
+    """Every decomposition pattern (the reference's -Qpattern values with its
+    own counts per pattern, and COST) and both join paradigms give the
+    reference's Q-mode counts: HPRD-15 and the scale-12 R-MAT queries the
+    reference's join path finished."""
+    ref = join_ref()
+    counts = ref["patterns"]["STAR" if pattern == "COST" else pattern]
+    g, hq, _ = gd.hprd()
+    hdg = api.DataGraph.from_graph(g)
+    rg = gen.make_graph("rmat", 2, scale=12, edge_factor=8, num_labels=32)
+    rdg = api.DataGraph.from_graph(rg)
+    cases = [(hdg, q, c, 4) for q, c in zip(hq, counts["hprd"])]
+    cases += [(rdg, gd.query_from_rec(e["query"]), c, 12)
+              for e, c in zip(ref["rmat12"]["queries"], counts["rmat12"])]
+    checked = 0
+    for dg, q, c, mu in cases:
+        if c is None:
+            continue
+        for jm in ("LEFTDEEP", "BUSHY"):
+            try:
+                r = api.match_join(engine, dg, q, "CFL_CFL_EXPLORE", max_unit_vertices=mu, pattern=pattern,
+                                   join_method=jm)
+            except PsmError as e:
+                # twin-twig covers of large queries need more than 32 units,
+                # or their relations outgrow the arena
+                assert pattern in ("TWINTWIG", "SEED") and ("units" in str(e) or "arena" in str(e)), e
+                continue
+            assert r.count == c, (pattern, jm, q.num_vertices)
+            checked += 1
+    hdg.close()
+    rdg.close()
+    assert checked >= 20
