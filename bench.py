@@ -486,6 +486,7 @@ def batched_mixed(args, local, graph=None, dg=None, flush=None):
     p_wall = time.perf_counter() - t
     clk = clocks.stop()
     p_dev = sum(r.prep_ms + r.enum_ms for r in plain)
+    p_enum = sum(r.enum_ms for r in plain)
     if [r.count for r in plain] != [r.count for r in res]:
         raise SystemExit("batched counts differ from the plain path")
     eng.close()
@@ -510,6 +511,11 @@ def batched_mixed(args, local, graph=None, dg=None, flush=None):
                                              for k, v in sorted(sizes.items())}},
             "speedup_vs_plain": value / (nq / (p_dev / 1e3)),
             "e2e_speedup_vs_plain": (nq * steps / wall) / (nq / p_wall),
+            # batching removes per-query preparation launches and overlaps
+            # enumeration tails; the enumeration work itself remains: the
+            # plain path's device time over its enumeration time is the
+            # speed-up from removing the preparation cost alone
+            "plain_enum_share": p_enum / p_dev, "plain_device_over_enum": p_dev / p_enum,
             "counts_equal_plain": True, "capped_queries": capped, "clocks": clk}
 
 
@@ -606,7 +612,7 @@ def serve_run(args, local):
     setup_s = time.time() - t
     lanes = args.lanes
     srv = api.Server(dg, w.method, cap=w.cap, time_limit=args.time_limit, lanes=lanes, max_batch=args.max_batch,
-                     lane_arena_bytes=(args.serve_budget_gb << 30) // lanes, full_gpu_lanes=True)
+                     lane_arena_bytes=(args.serve_budget_gb << 30) // lanes, full_gpu_lanes=not args.serve_share)
     clocks = ClockSampler(local).start()
     # warm-up, then saturation: everything queued at once
     for q in w.queries[: min(nq, 500)]:
@@ -623,17 +629,21 @@ def serve_run(args, local):
     base = min(r.ticket for r in res)
     counts = {r.ticket - base: r.count for r in res}
     sat_lat = [(r.done_ns - t0) / 1e6 for r in res]
-    # batches of the saturation run: (lane, start) -> size, prep / enum ms
+    # batches of the saturation run: (lane, start) -> size, wall span until
+    # the batch's last result
     batches = {}
     for r in res:
-        batches[(r.lane, r.start_ns)] = (r.batch_size, r.prep_ms, r.enum_ms)
+        k = (r.lane, r.start_ns)
+        size, end = batches.get(k, (r.batch_size, 0))
+        batches[k] = (size, max(end, r.done_ns))
     lane_busy = {}
-    for (ln, _), (_, pm, em) in batches.items():
-        lane_busy[ln] = lane_busy.get(ln, 0.0) + pm + em
+    for (ln, st), (_, end) in batches.items():
+        lane_busy[ln] = lane_busy.get(ln, 0.0) + (end - st) / 1e9
+    spans = [(end - st) / 1e6 for (_, st), (_, end) in batches.items()]
     batch_stats = {"batches": len(batches), "mean_batch": float(np.mean([b[0] for b in batches.values()])),
-                   "prep_ms_total": float(sum(b[1] for b in batches.values())),
-                   "enum_ms_total": float(sum(b[2] for b in batches.values())),
-                   "lane_device_busy_frac": {str(k): v / 1e3 / sat_span for k, v in sorted(lane_busy.items())}}
+                   "span_ms": {"p50": float(np.percentile(spans, 50)), "p99": float(np.percentile(spans, 99)),
+                               "max": float(max(spans))},
+                   "lane_busy_frac": {str(k): v / sat_span for k, v in sorted(lane_busy.items())}}
     loads = {}
     for load in args.serve_loads:
         rate = load * sat
@@ -680,7 +690,10 @@ def serve_run(args, local):
         bad = sum(1 for i, r in enumerate(pres) if r.count != counts[i])
         if bad:
             raise SystemExit(f"serving: {bad} counts differ from the plain path")
+        plat = [r.prep_ms + r.enum_ms for r in pres]
         plain = {"queries": len(sample), "value": len(sample) / p_dev, "e2e": len(sample) / p_wall,
+                 "latency_ms": {"p50": float(np.percentile(plat, 50)), "p99": float(np.percentile(plat, 99)),
+                                "max": float(max(plat))},
                  "unit": "queries/s", "served_saturation_vs_plain_e2e": sat / (len(sample) / p_wall),
                  "counts_equal_served": True}
     dg.close()
@@ -690,6 +703,7 @@ def serve_run(args, local):
                        "edges": w.graph.num_edges, "queries": nq,
                        "query_sizes": "{4,8,12,16,24,32} weighted .3/.25/.2/.1/.1/.05", "cap": w.cap,
                        "lanes": lanes, "max_batch": args.max_batch, "budget_gb": args.serve_budget_gb,
+                       "lane_grid": "1/lanes of the GPU" if args.serve_share else "whole GPU",
                        "setup_s": setup_s},
             "saturation_qps": sat, "saturation_span_s": sat_span,
             "saturation_latency_ms": {"p50": float(np.percentile(sat_lat, 50)),
@@ -735,6 +749,8 @@ def main():
     ap.add_argument("--lanes", type=int, default=4, help="serving lanes")
     ap.add_argument("--max-batch", type=int, default=64, help="serving batch limit")
     ap.add_argument("--serve-budget-gb", type=int, default=120, help="serving device-memory budget")
+    ap.add_argument("--serve-share", action="store_true",
+                    help="size each serving lane's grids to 1/lanes of the GPU (else every lane launches whole-GPU grids)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.workload != "plain":

@@ -551,52 +551,46 @@ __device__ __forceinline__ u32 cached_exclusions(const QState& q, u32 dl, u32 v,
 }
 
 __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 v, const WarpStack* ws, u64& bytes,
-                               u64& calls, bool* defer, u32 act, u32 G, u32 sub) {
-    // A group of G lanes shares the candidate: lane `sub` of the group walks
-    // entries sub, sub + G, ...; the group's leader (sub 0) adds the
-    // candidate's bytes, calls and exclusions. Per-lane counts may wrap
-    // below zero; the warp's sum of them is the candidates' total.
+                               u64& calls, bool* defer, u32 act) {
     const u32 nb = q.nbn[dl];
     const u32 dp = dl - 1;
-    const bool lead = sub == 0;
-    const u32 long_bm = min(LONG_BM_ROW, DEFER_BM_PER_LANE * act) * G;
-    const u32 long_row = min(LONG_ROW, max(2u, DEFER_ROW_PER_LANE * act)) * G;
+    const u32 long_bm = min(LONG_BM_ROW, DEFER_BM_PER_LANE * act);
+    const u32 long_row = min(LONG_ROW, max(2u, DEFER_ROW_PER_LANE * act));
     if (cached) {
         const u32 s = ws->clen[dl];
         const u32 k = q.crow[dl];
-        if (lead) bytes += 8ull * nb + 4ull * ws->csum[dl];
+        bytes += 8ull * nb + 4ull * ws->csum[dl];
         if (k == NO_ROW) {
-            if (!lead) return 0;
             calls += s;
             return s - cached_exclusions(q, dl, v, ws, false, 0, 0);
         }
         const u32 base = q.bn_tab[dl][k] + p;
         const u32 lo = q.P[base], hi = q.P[base + 1], r = hi - lo;
-        if (lead) bytes += 4ull * r;
+        bytes += 4ull * r;
         if (s == 0 || r == 0) return 0;
         u64 c = 0;
         if (walk_r_with_bitmap(ws, dl, r, s)) {
-            if (lead) calls += r;
+            calls += r;
             if (r > long_bm) {
                 *defer = true;
                 return 0;
             }
             const u32* bm = slot_bm(ws, dl);
-            for (u32 e = lo + sub; e < hi; e += G) c += bm_test(bm, __ldg(q.adj + e));
+            for (u32 e = lo; e < hi; ++e) c += bm_test(bm, __ldg(q.adj + e));
         } else {
-            if (lead) calls += min(s, r);
+            calls += min(s, r);
             if (min(s, r) > long_row) {
                 *defer = true;
                 return 0;
             }
             const u32* S = cache_list(q, ws, dl);
             if (r <= s) {
-                for (u32 e = lo + sub; e < hi; e += G) c += contains_rw(S, 0, s, __ldg(q.adj + e));
+                for (u32 e = lo; e < hi; ++e) c += contains_rw(S, 0, s, __ldg(q.adj + e));
             } else {
-                for (u32 i = sub; i < s; i += G) c += contains_u32(q.adj, lo, hi, S[i]);
+                for (u32 i = 0; i < s; ++i) c += contains_u32(q.adj, lo, hi, S[i]);
             }
         }
-        return lead ? c - cached_exclusions(q, dl, v, ws, true, lo, hi) : c;
+        return c - cached_exclusions(q, dl, v, ws, true, lo, hi);
     }
     u32 blo = 0, bhi = 0, blen = 0xFFFFFFFFu, bk = 0;
     u64 by = 0;
@@ -607,10 +601,8 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
         by += 8u + 4ull * (hi - lo);
         if (hi - lo < blen) blen = hi - lo, blo = lo, bhi = hi, bk = k;
     }
-    if (lead) {
-        bytes += by;
-        calls += blen;
-    }
+    bytes += by;
+    calls += blen;
     if (blen == 0) return 0;
     if (nb > 1 && blen > long_row) {
         *defer = true;
@@ -619,7 +611,6 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
     const u32 u = q.order[dl];
     const u32 same = q.same_mask[dl];
     if (nb == 1) {
-        if (!lead) return 0;
         u64 c = blen;
         u32 m = same;
         // the row of v's own depth holds v only through a self loop
@@ -634,7 +625,7 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
     }
     const u32* list = q.list[u];
     u64 c = 0;
-    for (u32 e = blo + sub; e < bhi; e += G) {
+    for (u32 e = blo; e < bhi; ++e) {
         const u32 x = __ldg(q.adj + e);
         bool ok = true;
         for (u32 k = 0; k < nb && ok; ++k) {
@@ -1069,31 +1060,16 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
                 const u32 p = valid ? (d == 0 ? idx : drv_elem(q, ws, d, idx)) : 0u;
                 const bool ok = d == 0 ? valid : chunk_accept(q, d, p, valid, ws, list_d);
                 const u32 v = ok ? list_d[p] : 0u;
-                const u32 bal = __ballot_sync(FULL_MASK, ok);
-                const u32 act = __popc(bal);
-                // G lanes per surviving candidate (the largest power of two
-                // with G x act <= 32): candidate ci goes to lanes
-                // [ci G, ci G + G), taken from the lane holding the ci-th
-                // set bit of the ballot
-                u32 G = 1;
-                while (G < 32u && 2u * G * act <= 32u) G <<= 1;
-                const u32 ci = lane / G, sub = lane & (G - 1u);
-                u32 src = 0;  // largest position with at most ci set bits below it
-#pragma unroll
-                for (u32 step = 16; step; step >>= 1)
-                    if (__popc(bal & ((1u << (src + step)) - 1u)) <= ci) src += step;
-                const bool has = ci < act;
-                const u32 pg = __shfl_sync(FULL_MASK, p, has ? src : 0u);
-                const u32 vg = __shfl_sync(FULL_MASK, v, has ? src : 0u);
-                if (has) c = lane_last_count(q, d + 1, cached, pg, vg, ws, bytes_l, calls_l, &defer, act, G, sub);
+                const u32 act = __popc(__ballot_sync(FULL_MASK, ok));
+                if (ok) c = lane_last_count(q, d + 1, cached, p, v, ws, bytes_l, calls_l, &defer, act);
                 count += warp_sum64(c);
-                // long intersections deferred by their groups: whole warp each
-                u32 dm = __ballot_sync(FULL_MASK, defer && sub == 0);
+                // long intersections deferred by their lanes: whole warp each
+                u32 dm = __ballot_sync(FULL_MASK, defer);
                 while (dm) {
-                    const u32 leader = __ffs(dm) - 1;
+                    const u32 src = __ffs(dm) - 1;
                     dm &= dm - 1;
-                    count += warp_last_count(q, d + 1, cached, __shfl_sync(FULL_MASK, pg, leader),
-                                             __shfl_sync(FULL_MASK, vg, leader), ws);
+                    count += warp_last_count(q, d + 1, cached, __shfl_sync(FULL_MASK, p, src),
+                                             __shfl_sync(FULL_MASK, v, src), ws);
                 }
                 calls += min(32u, end - cur);
                 __syncwarp();

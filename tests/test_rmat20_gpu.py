@@ -13,9 +13,10 @@ that:
   * every embedding the enumerator counts for a capped benchmark query is a
     valid, distinct embedding (emission mode, checked on the host), so a
     capped count cannot hide over-counting;
-  * uncapped counts of benchmark queries agree across both methods (different
-    candidates, tables and orders), with and without the enumerator's caches,
-    and between the plain and batched paths.
+  * uncapped counts above the cap (6- and 8-vertex queries of the batched
+    workload on this graph) agree across both methods (different candidates,
+    tables and orders), with and without the enumerator's caches, and
+    between the plain and batched paths.
 """
 import os
 
@@ -135,27 +136,30 @@ def test_capped_counts_are_distinct_valid_embeddings(pinned, graph, dev):
             valid_distinct(graph, q, emb)
 
 
-def test_uncapped_counts_agree_across_paths(pinned, dev):
-    """Without the cap the benchmark queries' counts exceed it. Where the
-    device finishes them in a few seconds, the count is the same under both
-    methods, without the enumerator's caches, and through the batched path."""
+def test_uncapped_counts_agree_across_paths(graph, dev):
+    """Without the cap, counts above it agree across paths. The batched
+    workload's 6- and 8-vertex queries on this graph (the reference does not
+    finish them within minutes) have counts from 1e9 to about 1e11, which the
+    device finishes in a second or two: the count is the same under both
+    methods (different candidates, tables and orders), without the
+    enumerator's caches, and through the batched path."""
+    from psm_benchmark_b200 import gen
     eng, dg = dev
     os.environ["PSM_ENUM_CACHE"] = "0"
     try:
         plain_eng = api.Engine(arena_bytes=8 << 30)
     finally:
         del os.environ["PSM_ENUM_CACHE"]
+    mixed = gen.batched(graph=graph)
     agreed = 0
     try:
-        for e in pinned["bench"]:
-            q = gd.query_from_rec(e["query"])
+        for q in [q for q in mixed.queries if q.num_vertices in (6, 8)][:60]:
             first = api.match(eng, dg, q, "CFL_CFL_EXPLORE", cap=0, time_limit=1.0)
-            if first.overtime:
+            if first.overtime or first.count <= 10**9:
                 continue
-            assert first.count > pinned["cap"]
             for m, en in (("GQL_GQL_GQL", eng), ("CFL_CFL_EXPLORE", plain_eng)):
                 r = api.match(en, dg, q, m, cap=0, time_limit=30.0)
-                assert not r.overtime and r.count == first.count, (e["index"], m)
+                assert not r.overtime and r.count == first.count, (q.num_vertices, m)
             b = api.match_batch(eng, dg, [q, q], "CFL_CFL_EXPLORE", cap=0, time_limit=30.0)
             assert [r.count for r in b] == [first.count] * 2
             agreed += 1
