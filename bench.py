@@ -598,6 +598,79 @@ def join_leg(args, local):
     print(json.dumps(line))
 
 
+def join4_leg(args, local):
+    """Config-4-shaped decomposition + join: R-MAT (edge factor 16, 64
+    Zipf(1.0) labels) at a reduced scale, 24-32-vertex random-walk queries,
+    the cost-based bounded decomposition (units <= 12 vertices) joined bushy,
+    each query under a time limit; counts checked against the plain path on
+    the same queries and, on a bounded sample, the reference's own join path
+    (-QorCandi Q)."""
+    _torch_setup(local)
+    from psm_benchmark_b200 import api, gen
+    w = gen.join(num_queries=args.join_queries, scale=args.join_scale)
+    eng = api.Engine(device=local, arena_bytes=max(args.arena_gb, 64) << 30)
+    dg = api.DataGraph.from_graph(w.graph)
+    rows = []
+    for i, q in enumerate(w.queries):
+        t = time.perf_counter()
+        try:
+            r = api.match_join(eng, dg, q, w.method, max_unit_vertices=12, pattern="COST", join_method="BUSHY",
+                               time_limit=args.join_limit)
+            jt = time.perf_counter() - t
+            jres = (r.count, r.prep_ms + r.enum_ms + r.join_ms, jt, len(r.units))
+        except Exception as e:  # time limit or arena: the query did not finish
+            jres = (None, None, time.perf_counter() - t, str(e)[:60])
+        p = api.match(eng, dg, q, w.method, cap=0, time_limit=args.join_limit)
+        rows.append({"i": i, "n": q.num_vertices, "join": jres, "plain": (None if p.overtime else p.count,
+                                                                         p.prep_ms + p.enum_ms)})
+    done = [r for r in rows if r["join"][0] is not None]
+    agree = sum(1 for r in done if r["plain"][0] is not None and r["plain"][0] == r["join"][0])
+    both = sum(1 for r in done if r["plain"][0] is not None)
+    if agree != both:
+        raise SystemExit("join counts differ from the plain path")
+    dev_s = sum(r["join"][1] for r in done) / 1e3
+    line = {"metric": "queries/sec (decomposition + hash-join path, config-4 shape)",
+            "value": len(done) / dev_s if dev_s else 0.0, "unit": "queries/s", "n_gpus": 1, "steps": 1,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic",
+            "config": {"workload": "join_rmat", "graph": f"R-MAT scale {args.join_scale}, edge factor 16, "
+                                                         "64 Zipf(1.0) labels",
+                       "edges": w.graph.num_edges, "queries": len(w.queries), "query_sizes": "24-32",
+                       "pattern": "COST (units <= 12), BUSHY", "time_limit_s": args.join_limit},
+            "finished": len(done), "counts_checked_vs_plain": both,
+            "plain_finished": sum(1 for r in rows if r["plain"][0] is not None),
+            "per_query": rows}
+    if args.cpu_baseline and ref_available():
+        tmp = Path(tempfile.mkdtemp(prefix="psmjoin4_"))
+        d = tmp / "a" / "b" / "c"
+        (d / "q").mkdir(parents=True)
+        gen.write_text(w.graph, d / "g.txt")
+        ref = []
+        for r in rows[: args.join_ref_queries]:
+            qp = d / "q" / f"q{r['i']}.txt"
+            w.queries[r["i"]].write_text(qp)
+            log = tmp / "log.txt"
+            if log.exists():
+                log.unlink()
+            subprocess.run([str(REF_BIN), "-d", str(d / "g.txt"), "-q", str(qp), "-num", "MAX", "-time_limit",
+                            str(int(args.join_limit)), "-OutputFile", str(log), "-QorCandi", "Q", "-Qpattern", "STAR",
+                            "-JoinMethod", "LEFTDEEP", "-threadnums", "1", "-BackMethods", w.method],
+                           capture_output=True, timeout=args.join_limit + 300)
+            text = log.read_text() if log.exists() else ""
+            c = re.findall(r"#Embeddings: (\d+)", text)
+            o = re.findall(r"Overtime: (\d+)", text)
+            t = re.findall(r"Total time \(seconds\): ([0-9.e+-]+)", text)
+            fin = bool(c and o and o[-1] == "0")
+            ref.append({"i": r["i"], "count": int(c[-1]) if fin else None, "total_s": float(t[-1]) if t else None})
+            if fin and r["join"][0] is not None and int(c[-1]) != r["join"][0]:
+                raise SystemExit(f"join count differs from the reference's (query {r['i']})")
+        line["reference"] = {"runs": ref, "finished": sum(1 for x in ref if x["count"] is not None),
+                             "note": "-QorCandi Q -Qpattern STAR -JoinMethod LEFTDEEP -threadnums 1"}
+    eng.close()
+    dg.close()
+    print(json.dumps(line))
+
+
 def serve_run(args, local):
     """Serving on R-MAT scale 24 (edge factor 16, 128 uniform labels): the
     request stream all at once (saturation), then as Poisson arrivals at 50,
@@ -738,7 +811,11 @@ def main():
     ap.add_argument("--no-legs", dest="legs", action="store_false",
                     help="leave out the batched_mixed and serve keys of the default line")
     ap.add_argument("--only", default="", help="comma-separated query indices (profiling runs)")
-    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "join", "serve"])
+    ap.add_argument("--workload", default="plain", choices=["plain", "batched", "join", "join4", "serve"])
+    ap.add_argument("--join-scale", type=int, default=14)
+    ap.add_argument("--join-queries", type=int, default=40)
+    ap.add_argument("--join-limit", type=float, default=20.0)
+    ap.add_argument("--join-ref-queries", type=int, default=8)
     ap.add_argument("--mixed-queries", type=int, default=2000)
     ap.add_argument("--mixed-steps", type=int, default=2)
     ap.add_argument("--serve-queries", type=int, default=50000)
@@ -759,7 +836,8 @@ def main():
                 print(json.dumps({"impl": args.impl, "unavailable": "the batched, join and serve workloads run on "
                                                                      "one GPU through this arm only"}))
             return
-        {"batched": batched_leg, "join": join_leg, "serve": serve_leg}[args.workload](args, dist_setup()[2])
+        {"batched": batched_leg, "join": join_leg, "join4": join4_leg,
+         "serve": serve_leg}[args.workload](args, dist_setup()[2])
         return
     if args.impl == "reference":
         reference_arm(args, world, rank)

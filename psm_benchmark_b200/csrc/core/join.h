@@ -4,7 +4,7 @@
 
 #include "psm_internal.h"
 
-#define PSM_JOIN_MAX_KEYS 16
+#define PSM_JOIN_MAX_KEYS PSM_MAXQ
 
 // What one join compares and writes. Columns are indices into rows.
 struct JoinSpec {
