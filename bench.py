@@ -713,10 +713,17 @@ def serve_run(args, local):
     for (ln, st), (_, end) in batches.items():
         lane_busy[ln] = lane_busy.get(ln, 0.0) + (end - st) / 1e9
     spans = [(end - st) / 1e6 for (_, st), (_, end) in batches.items()]
+    # idle time of a lane between its batches (last result to next start)
+    gaps = []
+    for ln in set(k[0] for k in batches):
+        seq = sorted((st, end) for (l2, st), (_, end) in batches.items() if l2 == ln)
+        gaps += [(b[0] - a[1]) / 1e6 for a, b in zip(seq, seq[1:])]
     batch_stats = {"batches": len(batches), "mean_batch": float(np.mean([b[0] for b in batches.values()])),
                    "span_ms": {"p50": float(np.percentile(spans, 50)), "p99": float(np.percentile(spans, 99)),
                                "max": float(max(spans))},
-                   "lane_busy_frac": {str(k): v / sat_span for k, v in sorted(lane_busy.items())}}
+                   "lane_busy_frac": {str(k): v / sat_span for k, v in sorted(lane_busy.items())},
+                   "lane_gap_ms": {"p50": float(np.percentile(gaps, 50)) if gaps else 0.0,
+                                   "max": float(max(gaps)) if gaps else 0.0}}
     loads = {}
     for load in args.serve_loads:
         rate = load * sat
