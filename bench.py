@@ -469,6 +469,11 @@ def batched_mixed(args, local, graph=None, dg=None, flush=None):
         return res, time.perf_counter() - t
 
     steps = args.mixed_steps
+    # the autotuner picks the batch settings on a sample of the workload
+    tune = None
+    if args.autotune:
+        tune = eng.autotune_batch(dg, w.queries[: args.tune_queries], w.method, cap=w.cap,
+                                  time_limit=args.time_limit, repeats=1)
     batched()
     clocks = ClockSampler(local).start()
     dev, wall, res = 0.0, 0.0, None
@@ -516,7 +521,9 @@ def batched_mixed(args, local, graph=None, dg=None, flush=None):
             # plain path's device time over its enumeration time is the
             # speed-up from removing the preparation cost alone
             "plain_enum_share": p_enum / p_dev, "plain_device_over_enum": p_dev / p_enum,
-            "counts_equal_plain": True, "capped_queries": capped, "clocks": clk}
+            "counts_equal_plain": True, "capped_queries": capped, "clocks": clk,
+            "autotune": ({"sample_queries": min(nq, args.tune_queries), "best": tune["best"], "tried": tune["tried"]}
+                         if tune else None)}
 
 
 def batched_leg(args, local):
@@ -825,6 +832,9 @@ def main():
     ap.add_argument("--join-ref-queries", type=int, default=8)
     ap.add_argument("--mixed-queries", type=int, default=2000)
     ap.add_argument("--mixed-steps", type=int, default=2)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="leave the batched path's settings at their defaults")
+    ap.add_argument("--tune-queries", type=int, default=300, help="sample of the mixed workload for the autotuner")
     ap.add_argument("--serve-queries", type=int, default=50000)
     ap.add_argument("--serve-scale", type=int, default=24)
     ap.add_argument("--serve-plain", type=int, default=2000,

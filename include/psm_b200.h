@@ -256,6 +256,30 @@ int psm_hash_join(psm_context* ctx, const uint32_t* r_rows, uint64_t r_n, uint32
 int psm_match_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, uint32_t nq,
                     const psm_options* opt, psm_result* results);
 
+/* Settings of a context's batched launches (psm_match_batch and the serving
+ * lanes; no counterpart in the reference). */
+#define PSM_TEAM_RULE 0     /* a cluster per query for small batches, a block per query for large ones */
+#define PSM_TEAM_BLOCK 1    /* one thread block prepares each query */
+#define PSM_TEAM_CLUSTER 2  /* one thread-block cluster prepares each query */
+typedef struct psm_batch_tuning {
+    uint32_t team;            /* PSM_TEAM_*: preparation team of a query */
+    uint32_t grabs_per_warp;  /* 1..64: how finely a query's initial work is cut, per enumeration warp */
+    uint32_t enum_quarters;   /* 1..4: enumeration grid in quarters of the co-resident blocks */
+    uint32_t reserved;
+    double ms;                /* psm_autotune_batch: device time of the sample under this setting */
+} psm_batch_tuning;
+int psm_context_set_batch_tuning(psm_context* ctx, const psm_batch_tuning* t);
+int psm_context_get_batch_tuning(psm_context* ctx, psm_batch_tuning* t);
+/* Autotuner of the batched path: runs the sample batch under every candidate
+ * setting (teams x grabs_per_warp {2, 8, 32} x enum_quarters {2, 4}), keeps
+ * the one with the least device time (the best of `repeats` runs after one
+ * warm-up), installs it in the context and returns it in *best; every
+ * setting tried is written to tried[0 .. *ntried) (up to tried_cap). The
+ * counts of every setting must be equal (PSM_ERR_INTERNAL otherwise). */
+int psm_autotune_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* sample, uint32_t n,
+                       const psm_options* opt, uint32_t repeats, psm_batch_tuning* best, psm_batch_tuning* tried,
+                       uint32_t tried_cap, uint32_t* ntried);
+
 /* ---- serving: request loop with continuous batching over a resident graph
  *      (no counterpart in the reference, which runs one query per process) ---- */
 typedef struct psm_server psm_server;

@@ -31,6 +31,30 @@ class Engine:
             N.lib().psm_context_free(self._h)
             self._h = C.c_void_p()
 
+    def batch_tuning(self) -> dict:
+        """Settings of this context's batched launches."""
+        t = N.BatchTuning()
+        N.check(N.lib().psm_context_get_batch_tuning(self._h, C.byref(t)))
+        return t.as_dict()
+
+    def set_batch_tuning(self, team: str = "RULE", grabs_per_warp: int = 8, enum_quarters: int = 4):
+        t = N.BatchTuning(N.TEAMS[team], int(grabs_per_warp), int(enum_quarters), 0, 0.0)
+        N.check(N.lib().psm_context_set_batch_tuning(self._h, C.byref(t)))
+
+    def autotune_batch(self, data, queries, method: str = "CFL_CFL_EXPLORE", cap: int = 0,
+                       time_limit: float = 60.0, repeats: int = 2) -> dict:
+        """Times the sample batch under every candidate setting, installs the
+        fastest in this context. Returns {"best": ..., "tried": [...]}."""
+        bufs = [_QueryBuf(q) for q in queries]
+        arr = (N.QueryDesc * len(bufs))(*[b.desc for b in bufs])
+        opt = options(method, cap, time_limit)
+        best = N.BatchTuning()
+        tried = (N.BatchTuning * 32)()
+        nt = C.c_uint32()
+        N.check(N.lib().psm_autotune_batch(self._h, data._h, arr, len(bufs), C.byref(opt), int(repeats),
+                                           C.byref(best), tried, 32, C.byref(nt)))
+        return {"best": best.as_dict(), "tried": [tried[i].as_dict() for i in range(nt.value)]}
+
     def __del__(self):
         try:
             self.close()

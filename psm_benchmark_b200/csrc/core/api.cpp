@@ -85,6 +85,10 @@ struct psm_context {
     int batch_cluster = 0;   // > 0: batched preparation by clusters of this many blocks, one query each
     int batch_clusters = 0;  // clusters of that launch
     int enum_blocks = 0;
+    // batched-path settings (psm_context_set_batch_tuning / psm_autotune_batch)
+    u32 tune_team = PSM_TEAM_RULE;   // preparation team of a batch
+    u32 tune_grabs = 8;              // initial work pieces per enumeration warp
+    u32 tune_quarters = 4;           // enumeration grid: quarters of the co-resident blocks
     cudaEvent_t ev[4]{};
     char* pinned = nullptr;  // pinned host staging of descriptors, states and results
     size_t pinned_bytes = 0;
@@ -187,7 +191,14 @@ int setup_query(psm_context* ctx, const psm_graph& g, const QDesc& d, const psm_
 }
 
 bool use_cluster_batch(const psm_context* ctx, u32 nq) {
-    return ctx->batch_cluster > 0 && nq <= 4u * (u32)ctx->batch_clusters;
+    if (ctx->batch_cluster <= 0 || ctx->tune_team == PSM_TEAM_BLOCK) return false;
+    if (ctx->tune_team == PSM_TEAM_CLUSTER) return true;
+    return nq <= 4u * (u32)ctx->batch_clusters;
+}
+
+// Enumeration grid of a batched launch (the tuning's share of the co-resident blocks).
+int batch_enum_blocks(const psm_context* ctx) {
+    return std::max(1, ctx->enum_blocks * (int)ctx->tune_quarters / 4);
 }
 
 u64 budget_ns(const psm_options& o) {
@@ -313,7 +324,8 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
     if (!prep_only)
         CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_enum_q, budget, opt.emit ? 1 : 0,
-                           ctx->enum_blocks, ctx->d_enum_cache, done, exit_keep, ctx->st));
+                           grid_team ? ctx->enum_blocks : batch_enum_blocks(ctx), ctx->d_enum_cache, done, exit_keep,
+                           ctx->st, grid_team ? 8u : ctx->tune_grabs));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     CK(psm_launch_gather(lay.d_q, nq, lay.d_res, ctx->st));
     if (poll) {
@@ -586,6 +598,74 @@ int psm_match_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* 
                     const psm_options* opt, psm_result* results) {
     if (!opt || !results) return fail(PSM_ERR_ARG, "null argument");
     return run_queries(ctx, g, qs, nq, *opt, false, results, nullptr);
+}
+
+int psm_context_set_batch_tuning(psm_context* ctx, const psm_batch_tuning* t) {
+    if (!ctx || !t) return fail(PSM_ERR_ARG, "null argument");
+    if (t->team > PSM_TEAM_CLUSTER || t->grabs_per_warp < 1 || t->grabs_per_warp > 64 || t->enum_quarters < 1 ||
+        t->enum_quarters > 4)
+        return fail(PSM_ERR_ARG, "tuning out of range");
+    if (t->team == PSM_TEAM_CLUSTER && ctx->batch_cluster <= 0)
+        return fail(PSM_ERR_ARG, "this context has no cluster preparation");
+    ctx->tune_team = t->team;
+    ctx->tune_grabs = t->grabs_per_warp;
+    ctx->tune_quarters = t->enum_quarters;
+    return PSM_OK;
+}
+
+int psm_context_get_batch_tuning(psm_context* ctx, psm_batch_tuning* t) {
+    if (!ctx || !t) return fail(PSM_ERR_ARG, "null argument");
+    memset(t, 0, sizeof(*t));
+    t->team = ctx->tune_team;
+    t->grabs_per_warp = ctx->tune_grabs;
+    t->enum_quarters = ctx->tune_quarters;
+    return PSM_OK;
+}
+
+int psm_autotune_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* sample, uint32_t n,
+                       const psm_options* opt, uint32_t repeats, psm_batch_tuning* best, psm_batch_tuning* tried,
+                       uint32_t tried_cap, uint32_t* ntried) {
+    if (!ctx || !g || !sample || n == 0 || !opt || !best) return fail(PSM_ERR_ARG, "null argument");
+    if (opt->emit) return fail(PSM_ERR_ARG, "the tuner counts; emit is not supported");
+    const psm_batch_tuning before{ctx->tune_team, ctx->tune_grabs, ctx->tune_quarters, 0, 0.0};
+    std::vector<psm_batch_tuning> cands;
+    std::vector<u32> teams{PSM_TEAM_BLOCK};
+    if (ctx->batch_cluster > 0) teams.push_back(PSM_TEAM_CLUSTER);
+    for (u32 team : teams)
+        for (u32 grabs : {2u, 8u, 32u})
+            for (u32 quarters : {2u, 4u}) cands.push_back({team, grabs, quarters, 0, 0.0});
+    std::vector<psm_result> res(n);
+    std::vector<u64> counts;
+    int best_i = -1;
+    for (size_t i = 0; i < cands.size(); ++i) {
+        psm_context_set_batch_tuning(ctx, &cands[i]);
+        double ms = 0;
+        for (u32 r = 0; r <= std::max(1u, repeats); ++r) {
+            int rc = run_queries(ctx, g, sample, n, *opt, false, res.data(), nullptr);
+            if (rc && rc != PSM_ERR_TIMEOUT) {
+                psm_context_set_batch_tuning(ctx, &before);
+                return rc;
+            }
+            const double t = res[0].prep_ms + res[0].enum_ms;
+            if (r == 1 || (r > 1 && t < ms)) ms = t;  // run 0 warms up
+        }
+        cands[i].ms = ms;
+        std::vector<u64> c(n);
+        for (u32 q = 0; q < n; ++q) c[q] = res[q].count;
+        if (counts.empty()) {
+            counts = c;
+        } else if (c != counts) {
+            psm_context_set_batch_tuning(ctx, &before);
+            return fail(PSM_ERR_INTERNAL, "counts differ between batch settings");
+        }
+        if (best_i < 0 || ms < cands[best_i].ms) best_i = (int)i;
+    }
+    *best = cands[best_i];
+    psm_context_set_batch_tuning(ctx, best);
+    if (ntried) *ntried = (u32)std::min<size_t>(cands.size(), tried ? tried_cap : 0);
+    if (tried)
+        for (u32 i = 0; i < cands.size() && i < tried_cap; ++i) tried[i] = cands[i];
+    return PSM_OK;
 }
 
 int psm_run_create(psm_context* ctx, const psm_graph* g, const psm_query_desc* q, const psm_options* opt,

@@ -1394,7 +1394,8 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 3) enum_kernel(DevGraph 
 // queries of four or more vertices, roots otherwise), their prefix in grabs,
 // the per-query task counts and the queue's sequence numbers.
 __global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, u32* grab_prefix, PoolInfo* pools,
-                                 u32* remaining, QDoneRec* done, u32 exit_keep, u32 total_warps, u64 budget_ns) {
+                                 u32* remaining, QDoneRec* done, u32 exit_keep, u32 total_warps, u64 budget_ns,
+                                 u32 grabs_per_warp) {
     __shared__ u32 s_carry;
     __shared__ u32 wt[32];
     if (threadIdx.x == 0) s_carry = 0;
@@ -1419,8 +1420,9 @@ __global__ void enum_init_kernel(QState* qs, u32 nq, EnumCtl* ctl, Slot* slots, 
                     pi.first = 0;
                     pi.units = q.root_cnt;
                 }
-                // about 8 grabs per warp for a lone query; never below one unit
-                const u32 target = total_warps * 8u;
+                // about grabs_per_warp grabs per warp for a lone query (8 by
+                // default); never below one unit
+                const u32 target = total_warps * grabs_per_warp;
                 pi.grab = max(1u, pi.units / max(1u, target));
                 grabs = (pi.units + pi.grab - 1) / pi.grab;
             }
@@ -1507,14 +1509,15 @@ size_t psm_enum_query_bytes(u32 nq) {
 }
 
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
-                            int emit, int blocks, u32* cache, QDoneRec* done, u32 exit_keep, cudaStream_t st) {
+                            int emit, int blocks, u32* cache, QDoneRec* done, u32 exit_keep, cudaStream_t st,
+                            u32 grabs_per_warp) {
     EnumCtl* ctl = (EnumCtl*)scratch;
     Slot* slots = (Slot*)((char*)scratch + align16(sizeof(EnumCtl)));
     u32* grab_prefix = (u32*)query_scratch;
     PoolInfo* pools = (PoolInfo*)((char*)query_scratch + align16(sizeof(u32) * (nq + 1)));
     u32* remaining = (u32*)((char*)pools + align16(sizeof(PoolInfo) * nq));
     enum_init_kernel<<<1, 1024, 0, st>>>(qs, nq, ctl, slots, grab_prefix, pools, remaining, done, exit_keep,
-                                         (u32)blocks * WARPS_PER_BLOCK, budget_ns);
+                                         (u32)blocks * WARPS_PER_BLOCK, budget_ns, max(1u, grabs_per_warp));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     enum_kernel<<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, grab_prefix, pools, emit, cache);

@@ -92,8 +92,11 @@ size_t psm_enum_cache_bytes(int blocks);
 // prefix-intersection caches, or null to run without them. done: per-query
 // completion records in host-mapped memory (device address), or null.
 // exit_keep > 0 lets idle warps beyond that many leave once no work is left.
+// grabs_per_warp: how finely each query's initial work is cut (about that
+// many pieces per warp of the launch for a lone query).
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
-                            int emit, int blocks, u32* cache, QDoneRec* done, u32 exit_keep, cudaStream_t st);
+                            int emit, int blocks, u32* cache, QDoneRec* done, u32 exit_keep, cudaStream_t st,
+                            u32 grabs_per_warp = 8);
 cudaError_t psm_enum_max_blocks(int* blocks);
 cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st);
 cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st);

@@ -25,6 +25,7 @@ EXPORTS = [
     "psm_context_create", "psm_context_free",
     "psm_match", "psm_run_create", "psm_run_candidates", "psm_run_table", "psm_run_order",
     "psm_run_embeddings", "psm_run_free", "psm_match_batch", "psm_run_recount_noalloc",
+    "psm_context_set_batch_tuning", "psm_context_get_batch_tuning", "psm_autotune_batch",
     "psm_match_join", "psm_query_decompose", "psm_hash_join", "psm_match_join_ex", "psm_query_decompose_ex",
     "psm_server_create", "psm_server_submit", "psm_server_poll", "psm_server_pending", "psm_server_estimate",
     "psm_server_clock_ns", "psm_server_destroy",
@@ -72,6 +73,19 @@ class RequestResult(C.Structure):
                 ("batch_size", C.c_uint32), ("lane", C.c_uint32), ("prep_ms", C.c_double), ("enum_ms", C.c_double)]
 
 
+TEAMS = {"RULE": 0, "BLOCK": 1, "CLUSTER": 2}
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("team", C.c_uint32), ("grabs_per_warp", C.c_uint32), ("enum_quarters", C.c_uint32),
+                ("reserved", C.c_uint32), ("ms", C.c_double)]
+
+    def as_dict(self):
+        team = {v: k for k, v in TEAMS.items()}[self.team]
+        return {"team": team, "grabs_per_warp": self.grabs_per_warp, "enum_quarters": self.enum_quarters,
+                "ms": self.ms}
+
+
 SPLIT_PATTERNS = {"BOUNDED": 0, "STAR": 1, "TWINTWIG": 2, "SEED": 3, "SKETCHTREE": 4, "COST": 5}
 JOIN_METHODS = {"LEFTDEEP": 0, "BUSHY": 1}
 
@@ -117,6 +131,10 @@ def lib():
         "psm_run_order": ([vp, u32p, u32p], C.c_int),
         "psm_run_embeddings": ([vp, u32p, C.c_uint64, C.POINTER(C.c_uint64)], C.c_int),
         "psm_run_free": ([vp], None),
+        "psm_context_set_batch_tuning": ([vp, C.POINTER(BatchTuning)], C.c_int),
+        "psm_context_get_batch_tuning": ([vp, C.POINTER(BatchTuning)], C.c_int),
+        "psm_autotune_batch": ([vp, vp, C.POINTER(QueryDesc), C.c_uint32, C.POINTER(Options), C.c_uint32,
+                                C.POINTER(BatchTuning), C.POINTER(BatchTuning), C.c_uint32, u32p], C.c_int),
         "psm_match_batch": ([vp, vp, C.POINTER(QueryDesc), C.c_uint32, C.POINTER(Options), C.POINTER(Result)],
                             C.c_int),
         "psm_run_recount_noalloc": ([vp, C.c_uint64, C.c_double, C.POINTER(C.c_uint64), u32p], C.c_int),
