@@ -1300,6 +1300,32 @@ __device__ bool take_initial(EnumCtl* ctl, const u32* grab_prefix, const PoolInf
         else
             hi = mid;
     }
+    // A stopped query (cap reached, time limit) would still hand out every
+    // grab left in its pool, one ticket and three counter updates each, and
+    // the launch ends only after the last of them: the warp that meets a
+    // stopped query claims the rest of its grabs in one step instead. The
+    // claimed grabs never run, so they leave the query's remaining count;
+    // its own grab r still holds the query open, and whoever claims the
+    // pool's last grab releases the pool's token.
+    if (warp_ld_volatile_u32(&qs[lo].stop)) {
+        if (lane == 0) {
+            const u32 end = grab_prefix[lo + 1];
+            u32 cur = ld_volatile_u32(&ctl->ticket);
+            while (cur < end) {
+                const u32 prev = atomicCAS(&ctl->ticket, cur, end);
+                if (prev == cur) {
+                    atomicSub(&ctl->remaining[lo], end - cur);
+                    if (end == ctl->total_grabs) {
+                        __threadfence();
+                        atomicAdd(&ctl->pending, (unsigned long long)-1ll);
+                    }
+                    break;
+                }
+                cur = prev;
+            }
+        }
+        __syncwarp();
+    }
     const PoolInfo& pi = pools[lo];
     const u32 j = r - grab_prefix[lo];
     const u32 ub = j * pi.grab, ue = min(pi.units, ub + pi.grab);
