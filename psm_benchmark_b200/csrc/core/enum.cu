@@ -987,12 +987,12 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
             }
         }
     }
-    // Far from the cap a warp publishes every 64 K embeddings. Once its own
+    // Far from the cap a warp publishes every 16 K embeddings. Once its own
     // publish shows the query within reach of the cap (every warp's
     // unpublished share, twice over, could cross it), it publishes every 1 K:
     // the query then stops close to the cap instead of up to a share per warp
     // beyond it. Only lane 0 reads and writes near_q.
-    if (lane == 0 && count >= (ws->near_q == qi ? (1ull << 10) : (1ull << 16))) {
+    if (lane == 0 && count >= (ws->near_q == qi ? (1ull << 10) : (1ull << 14))) {
         unsigned long long old = atomicAdd((unsigned long long*)&q.count, count);
         if (q.cap) {
             const u64 total = old + count;
