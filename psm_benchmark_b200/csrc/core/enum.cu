@@ -252,6 +252,12 @@ __device__ bool ensure_cache(const QState& q, u32 d, WarpStack* ws, u64& bytes) 
         const u32 rest = cm & ~(1u << best);
         u32 n = 0;
         for (u32 j = 0; j < blen; j += 32) {
+            // a stopped query's long intersections end early: the cache is
+            // then not kept (the level falls back to the table rows)
+            if (j && (j & 4095u) == 0 && warp_ld_volatile_u32(&q.stop)) {
+                over = true;
+                break;
+            }
             bool ok = j + lane < blen;
             const u32 x = ok ? __ldg(q.adj + blo + j + lane) : 0u;
             for (u32 m = rest; m && ok; m &= m - 1) {
@@ -665,6 +671,9 @@ __device__ u64 warp_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
         if (walk_r_with_bitmap(ws, dl, r, s)) {
             const u32* bm = slot_bm(ws, dl);
             for (u32 e0 = lo; e0 < hi; e0 += 32) {
+                // a stopped query's hub-row walk ends early and counts
+                // nothing (its count is final or partial anyway)
+                if (((e0 - lo) & 8191u) == 8160u && warp_ld_volatile_u32(&q.stop)) return 0;
                 const u32 e = e0 + lane;
                 const bool ok = e < hi && bm_test(bm, __ldg(q.adj + e));
                 c += __popc(__ballot_sync(FULL_MASK, ok));
@@ -758,6 +767,7 @@ __device__ __forceinline__ MemoOut memo_count(const QState& q, u32 d, WarpStack*
     };
     // sum of w(x) over S_l \ V
     u64 a = 0;
+    bool cut = false;
     for (u32 i = lane; i < sl; i += 32) {
         const u32 x = Sl[i];
         if (in_v(x)) continue;
@@ -765,7 +775,16 @@ __device__ __forceinline__ MemoOut memo_count(const QState& q, u32 d, WarpStack*
         if (e == 0) {
             const u32 lo = q.P[q.memo_tab + x], hi = q.P[q.memo_tab + x + 1];
             u32 w = 0;
-            for (u32 k = lo; k < hi; ++k) w += bm_test(bmd, __ldg(q.adj + k));
+            for (u32 k = lo; k < hi; ++k) {
+                // a stopped query ends long row walks early (per lane: no
+                // warp-wide primitive inside this divergent loop)
+                if (((k - lo) & 2047u) == 2047u && ld_volatile_u32(&q.stop)) {
+                    cut = true;
+                    break;
+                }
+                w += bm_test(bmd, __ldg(q.adj + k));
+            }
+            if (cut) break;
             e = w + 1;
             memo[x] = e;
         }
@@ -806,6 +825,8 @@ __device__ __forceinline__ MemoOut memo_count(const QState& q, u32 d, WarpStack*
     ru = warp_sum64(ru);
     nu = warp_sum64(nu);
     const u64 accepted = sd - nu;
+    // a level cut short by the stop counts nothing
+    if (__any_sync(FULL_MASK, cut)) return MemoOut{0, 0, 0};
     return MemoOut{a - b, accepted * (8ull * q.nbn[l] + 4ull * ws->csum[l]) + 4ull * (ws->rsum - ru), accepted};
 }
 
