@@ -826,10 +826,10 @@ def main():
                     help="leave out the batched_mixed and serve keys of the default line")
     ap.add_argument("--only", default="", help="comma-separated query indices (profiling runs)")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "join", "join4", "serve"])
-    ap.add_argument("--join-scale", type=int, default=14)
-    ap.add_argument("--join-queries", type=int, default=40)
-    ap.add_argument("--join-limit", type=float, default=20.0)
-    ap.add_argument("--join-ref-queries", type=int, default=8)
+    ap.add_argument("--join-scale", type=int, default=11)
+    ap.add_argument("--join-queries", type=int, default=12)
+    ap.add_argument("--join-limit", type=float, default=5.0)
+    ap.add_argument("--join-ref-queries", type=int, default=6)
     ap.add_argument("--mixed-queries", type=int, default=2000)
     ap.add_argument("--mixed-steps", type=int, default=2)
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
