@@ -32,6 +32,15 @@ def test_undefined_split_mode_is_rejected(cli, tmp_path):
     assert log.read_text() == "[Thread 1] Error: The split mode is not defined.\n"
 
 
+def test_undefined_query_pattern_is_rejected(cli, tmp_path):
+    log = tmp_path / "out.log"
+    p = run(cli, ["-d", "x", "-q", "y", "-QorCandi", "Q", "-Qpattern", "CHAIN", "-OutputFile", str(log)])
+    assert p.returncode == 1
+    assert log.read_text() == "[Thread 1] Error: The split pattern 'CHAIN' is not defined.\n"
+    p = run(cli, ["-d", "x", "-q", "y", "-QorCandi", "Q", "-JoinMethod", "RIGHTDEEP", "-OutputFile", str(log)])
+    assert p.returncode == 1
+
+
 def test_missing_graph_files(cli, tmp_path):
     p = run(cli, ["-d", str(tmp_path / "missing.txt"), "-q", str(tmp_path / "q.txt"), "-QorCandi", "C"])
     assert p.returncode == 1
@@ -116,3 +125,24 @@ def test_hprd_counts_through_cli_q_mode(cli, tmp_path):
         assert int(blocks[0]["#Embeddings"]) == counts[i]
         assert blocks[0]["QuerySplit Pattern"] == "STAR"
         assert int(re.search(r"subgraph count == (\d+)", text).group(1)) >= 2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("pattern,join", [("SKETCHTREE", "LEFTDEEP"), ("TWINTWIG", "BUSHY"), ("COST", "BUSHY")])
+def test_q_mode_patterns_through_cli(cli, tmp_path, pattern, join):
+    """-Qpattern / -JoinMethod choose the decomposition and join tree; the
+    count is the reference's for every choice."""
+    g, qs, counts = hprd()
+    data = tmp_path / "d.txt"
+    g.write_text(data)
+    for i in (1, 4):
+        qf = tmp_path / f"q{i}.txt"
+        qs[i].write_text(qf)
+        log = tmp_path / f"q{i}_{pattern}.log"
+        p = run(cli, ["-d", str(data), "-q", str(qf), "-QorCandi", "Q", "-Qpattern", pattern, "-JoinMethod", join,
+                      "-threadnums", "1", "-OutputFile", str(log), "-BackMethods", "CFL_CFL_EXPLORE", "-max_unit", "4"])
+        assert p.returncode == 0, p.stderr
+        blocks = parse_blocks(log.read_text())
+        assert int(blocks[0]["#Embeddings"]) == counts[i]
+        assert blocks[0]["QuerySplit Pattern"] == pattern
+        assert blocks[0]["Join Paradigm"] == join
