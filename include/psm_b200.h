@@ -229,7 +229,8 @@ int psm_match_join_ex(psm_context* ctx, const psm_graph* g, const psm_query_desc
  * card model with data_vertices / data_edges): unit_masks[PSM_MAX_UNITS];
  * the plan as binary joins in execution order, join_ops[2 * j] and
  * join_ops[2 * j + 1] naming the operands of join j (a unit k < num_units,
- * or num_units + i = the result of join i). */
+ * or num_units + i = the result of join i); join_ops needs room for
+ * 2 * (PSM_MAX_UNITS - 1) entries (num_joins <= PSM_MAX_UNITS - 1). */
 int psm_query_decompose_ex(const psm_query_desc* q, const psm_join_options* jo, double data_vertices,
                            double data_edges, uint32_t* num_units, uint32_t* unit_masks, uint32_t* num_joins,
                            uint32_t* join_ops);
