@@ -262,21 +262,34 @@ int psm_match_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* 
 #define PSM_TEAM_RULE 0     /* a cluster per query for small batches, a block per query for large ones */
 #define PSM_TEAM_BLOCK 1    /* one thread block prepares each query */
 #define PSM_TEAM_CLUSTER 2  /* one thread-block cluster prepares each query */
+/* Intersection variants of the enumerator (the reference's
+ * ComputeSetIntersection::ComputeCandidates picks galloping for skewed
+ * pairs and a merge for balanced ones, utility/computesetintersection.cpp:5-30).
+ * They change the work, never the counts. */
+#define PSM_ISECT_BINARY 0  /* binary search of every entry of the shorter array, whole range (the
+                               default of a new context: the fastest on every workload measured) */
+#define PSM_ISECT_AUTO 1    /* per intersection, by its dependent loads: warp merge path for balanced
+                               arrays, binary search of the shorter array in the longer one for skewed
+                               ones, a two-cursor merge or a shrinking search for one lane's walk */
+#define PSM_ISECT_MERGE 2   /* merge wherever both arrays are non-empty */
 typedef struct psm_batch_tuning {
     uint32_t team;            /* PSM_TEAM_*: preparation team of a query */
     uint32_t grabs_per_warp;  /* 1..64: how finely a query's initial work is cut, per enumeration warp */
     uint32_t enum_quarters;   /* 1..4: enumeration grid in quarters of the co-resident blocks */
-    uint32_t reserved;
+    uint32_t intersect;       /* PSM_ISECT_*: every enumeration launch of the context (plain, batched,
+                                 join units, serving lanes) */
     double ms;                /* psm_autotune_batch: device time of the sample under this setting */
 } psm_batch_tuning;
 int psm_context_set_batch_tuning(psm_context* ctx, const psm_batch_tuning* t);
 int psm_context_get_batch_tuning(psm_context* ctx, psm_batch_tuning* t);
 /* Autotuner of the batched path: runs the sample batch under every candidate
- * setting (teams x grabs_per_warp {2, 8, 32} x enum_quarters {2, 4}), keeps
- * the one with the least device time (the best of `repeats` runs after one
- * warm-up), installs it in the context and returns it in *best; every
- * setting tried is written to tried[0 .. *ntried) (up to tried_cap). The
- * counts of every setting must be equal (PSM_ERR_INTERNAL otherwise). */
+ * setting (teams x grabs_per_warp {2, 8, 32} x enum_quarters {2, 4} under the
+ * installed intersection variant, then the other intersection variants under
+ * the best of those), keeps the one with the least device time (the best of
+ * `repeats` runs after one warm-up), installs it in the context and returns
+ * it in *best; every setting tried is written to tried[0 .. *ntried) (up to
+ * tried_cap). The counts of every setting must be equal (PSM_ERR_INTERNAL
+ * otherwise). */
 int psm_autotune_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* sample, uint32_t n,
                        const psm_options* opt, uint32_t repeats, psm_batch_tuning* best, psm_batch_tuning* tried,
                        uint32_t tried_cap, uint32_t* ntried);
@@ -317,8 +330,24 @@ int psm_server_pending(psm_server* s, uint64_t* queued, uint64_t* running);
 /* The device memory a request is admitted with, and a lane's budget. */
 int psm_server_estimate(psm_server* s, const psm_query_desc* q, uint64_t* bytes, uint64_t* lane_budget);
 uint64_t psm_server_clock_ns(void);
+/* Settings of every lane's batches (psm_batch_tuning, e.g. from
+ * psm_autotune_batch on a context of the same device): each lane applies them
+ * before its next batch. */
+int psm_server_set_batch_tuning(psm_server* s, const psm_batch_tuning* t);
 /* Finishes the running batches and stops; queued requests are dropped. */
 void psm_server_destroy(psm_server* s);
+
+/* ---- self-check of the enumerator's intersection primitives (test support;
+ *      no counterpart in the reference) ----
+ * One warp on the current device intersects the ascending arrays a[0, na)
+ * and b[0, nb) (distinct values below 0xFFFFFFFF each) in every form the
+ * enumerator uses: counts[0] = |a ∩ b| by warp merge path, counts[1] by one
+ * lane's two-cursor merge, counts[2] by one lane's search, counts[3] = the
+ * entries of the merge path with output written to list[0, cap) in
+ * ascending order, counts[4] = 1 when they would have exceeded cap. With
+ * filter != 0, counts[0] and the list keep only values not divisible by 3. */
+int psm_intersect_check(const uint32_t* a, uint32_t na, const uint32_t* b, uint32_t nb, uint32_t cap,
+                        uint32_t filter, uint32_t* counts, uint32_t* list);
 #ifdef __cplusplus
 }
 #endif

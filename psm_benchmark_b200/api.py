@@ -32,13 +32,15 @@ class Engine:
             self._h = C.c_void_p()
 
     def batch_tuning(self) -> dict:
-        """Settings of this context's batched launches."""
+        """Settings of this context's batched launches (the intersection
+        variant applies to every enumeration launch of the context)."""
         t = N.BatchTuning()
         N.check(N.lib().psm_context_get_batch_tuning(self._h, C.byref(t)))
         return t.as_dict()
 
-    def set_batch_tuning(self, team: str = "RULE", grabs_per_warp: int = 8, enum_quarters: int = 4):
-        t = N.BatchTuning(N.TEAMS[team], int(grabs_per_warp), int(enum_quarters), 0, 0.0)
+    def set_batch_tuning(self, team: str = "RULE", grabs_per_warp: int = 8, enum_quarters: int = 4,
+                         intersect: str = "BINARY"):
+        t = N.BatchTuning(N.TEAMS[team], int(grabs_per_warp), int(enum_quarters), N.INTERSECTS[intersect], 0.0)
         N.check(N.lib().psm_context_set_batch_tuning(self._h, C.byref(t)))
 
     def autotune_batch(self, data, queries, method: str = "CFL_CFL_EXPLORE", cap: int = 0,
@@ -378,6 +380,13 @@ class Server:
         t = C.c_uint64()
         N.check(N.lib().psm_server_submit(self._h, C.byref(qb.desc), C.byref(t)))
         return t.value
+
+    def set_batch_tuning(self, team: str = "RULE", grabs_per_warp: int = 8, enum_quarters: int = 4,
+                         intersect: str = "BINARY"):
+        """Settings of every lane's batches (as Engine.set_batch_tuning, e.g.
+        the best of Engine.autotune_batch), applied before each lane's next batch."""
+        t = N.BatchTuning(N.TEAMS[team], int(grabs_per_warp), int(enum_quarters), N.INTERSECTS[intersect], 0.0)
+        N.check(N.lib().psm_server_set_batch_tuning(self._h, C.byref(t)))
 
     def estimate(self, query: Graph):
         qb = _QueryBuf(query)

@@ -89,6 +89,7 @@ struct psm_context {
     u32 tune_team = PSM_TEAM_RULE;   // preparation team of a batch
     u32 tune_grabs = 8;              // initial work pieces per enumeration warp
     u32 tune_quarters = 4;           // enumeration grid: quarters of the co-resident blocks
+    u32 tune_isect = PSM_ISECT_BINARY;  // intersection variant of every enumeration launch
     cudaEvent_t ev[4]{};
     char* pinned = nullptr;  // pinned host staging of descriptors, states and results
     size_t pinned_bytes = 0;
@@ -127,6 +128,7 @@ int psm_run_internals(psm_run* r, RunInternals* out) {
     out->enum_blocks = r->ctx->enum_blocks;
     out->emit = r->hq.emit_buf != nullptr;
     out->prep_status = r->hq.status;
+    out->isect = r->ctx->tune_isect;
     return PSM_OK;
 }
 
@@ -325,7 +327,7 @@ int run_queries(psm_context* ctx, const psm_graph* g, const psm_query_desc* qs, 
     if (!prep_only)
         CK(psm_launch_enum(g->dev, lay.d_q, nq, ctx->d_enum_scratch, lay.d_enum_q, budget, opt.emit ? 1 : 0,
                            grid_team ? ctx->enum_blocks : batch_enum_blocks(ctx), ctx->d_enum_cache, done, exit_keep,
-                           ctx->st, grid_team ? 8u : ctx->tune_grabs));
+                           ctx->st, grid_team ? 8u : ctx->tune_grabs, ctx->tune_isect));
     CK(cudaEventRecord(ctx->ev[2], ctx->st));
     CK(psm_launch_gather(lay.d_q, nq, lay.d_res, ctx->st));
     if (poll) {
@@ -600,16 +602,27 @@ int psm_match_batch(psm_context* ctx, const psm_graph* g, const psm_query_desc* 
     return run_queries(ctx, g, qs, nq, *opt, false, results, nullptr);
 }
 
-int psm_context_set_batch_tuning(psm_context* ctx, const psm_batch_tuning* t) {
+}  // extern "C"
+
+int psm_batch_tuning_check(const psm_context* ctx, const psm_batch_tuning* t) {
     if (!ctx || !t) return fail(PSM_ERR_ARG, "null argument");
     if (t->team > PSM_TEAM_CLUSTER || t->grabs_per_warp < 1 || t->grabs_per_warp > 64 || t->enum_quarters < 1 ||
-        t->enum_quarters > 4)
+        t->enum_quarters > 4 || t->intersect > PSM_ISECT_MERGE)
         return fail(PSM_ERR_ARG, "tuning out of range");
     if (t->team == PSM_TEAM_CLUSTER && ctx->batch_cluster <= 0)
         return fail(PSM_ERR_ARG, "this context has no cluster preparation");
+    return PSM_OK;
+}
+
+extern "C" {
+
+int psm_context_set_batch_tuning(psm_context* ctx, const psm_batch_tuning* t) {
+    int rc = psm_batch_tuning_check(ctx, t);
+    if (rc) return rc;
     ctx->tune_team = t->team;
     ctx->tune_grabs = t->grabs_per_warp;
     ctx->tune_quarters = t->enum_quarters;
+    ctx->tune_isect = t->intersect;
     return PSM_OK;
 }
 
@@ -619,6 +632,7 @@ int psm_context_get_batch_tuning(psm_context* ctx, psm_batch_tuning* t) {
     t->team = ctx->tune_team;
     t->grabs_per_warp = ctx->tune_grabs;
     t->enum_quarters = ctx->tune_quarters;
+    t->intersect = ctx->tune_isect;
     return PSM_OK;
 }
 
@@ -627,38 +641,59 @@ int psm_autotune_batch(psm_context* ctx, const psm_graph* g, const psm_query_des
                        uint32_t tried_cap, uint32_t* ntried) {
     if (!ctx || !g || !sample || n == 0 || !opt || !best) return fail(PSM_ERR_ARG, "null argument");
     if (opt->emit) return fail(PSM_ERR_ARG, "the tuner counts; emit is not supported");
-    const psm_batch_tuning before{ctx->tune_team, ctx->tune_grabs, ctx->tune_quarters, 0, 0.0};
+    const psm_batch_tuning before{ctx->tune_team, ctx->tune_grabs, ctx->tune_quarters, ctx->tune_isect, 0.0};
     std::vector<psm_batch_tuning> cands;
-    std::vector<u32> teams{PSM_TEAM_BLOCK};
-    if (ctx->batch_cluster > 0) teams.push_back(PSM_TEAM_CLUSTER);
-    for (u32 team : teams)
-        for (u32 grabs : {2u, 8u, 32u})
-            for (u32 quarters : {2u, 4u}) cands.push_back({team, grabs, quarters, 0, 0.0});
     std::vector<psm_result> res(n);
     std::vector<u64> counts;
     int best_i = -1;
-    for (size_t i = 0; i < cands.size(); ++i) {
+    // times the sample under cands[i] (run 0 warms up, then the best of
+    // `repeats`); every setting must count the same embeddings
+    auto measure = [&](size_t i) -> int {
         psm_context_set_batch_tuning(ctx, &cands[i]);
         double ms = 0;
         for (u32 r = 0; r <= std::max(1u, repeats); ++r) {
             int rc = run_queries(ctx, g, sample, n, *opt, false, res.data(), nullptr);
-            if (rc && rc != PSM_ERR_TIMEOUT) {
-                psm_context_set_batch_tuning(ctx, &before);
-                return rc;
-            }
+            if (rc && rc != PSM_ERR_TIMEOUT) return rc;
             const double t = res[0].prep_ms + res[0].enum_ms;
-            if (r == 1 || (r > 1 && t < ms)) ms = t;  // run 0 warms up
+            if (r == 1 || (r > 1 && t < ms)) ms = t;
         }
         cands[i].ms = ms;
         std::vector<u64> c(n);
         for (u32 q = 0; q < n; ++q) c[q] = res[q].count;
-        if (counts.empty()) {
+        if (counts.empty())
             counts = c;
-        } else if (c != counts) {
-            psm_context_set_batch_tuning(ctx, &before);
+        else if (c != counts)
             return fail(PSM_ERR_INTERNAL, "counts differ between batch settings");
-        }
         if (best_i < 0 || ms < cands[best_i].ms) best_i = (int)i;
+        return PSM_OK;
+    };
+    // stage 1: preparation team x work pieces per warp x enumeration grid,
+    // under the installed intersection variant
+    std::vector<u32> teams{PSM_TEAM_BLOCK};
+    if (ctx->batch_cluster > 0) teams.push_back(PSM_TEAM_CLUSTER);
+    for (u32 team : teams)
+        for (u32 grabs : {2u, 8u, 32u})
+            for (u32 quarters : {2u, 4u}) cands.push_back({team, grabs, quarters, before.intersect, 0.0});
+    const size_t stage1 = cands.size();
+    for (size_t i = 0; i < stage1; ++i) {
+        int rc = measure(i);
+        if (rc) {
+            psm_context_set_batch_tuning(ctx, &before);
+            return rc;
+        }
+    }
+    // stage 2: the other intersection variants under stage 1's best setting
+    for (u32 v : {(u32)PSM_ISECT_AUTO, (u32)PSM_ISECT_BINARY, (u32)PSM_ISECT_MERGE}) {
+        if (v == before.intersect) continue;
+        psm_batch_tuning c = cands[best_i];
+        c.intersect = v;
+        c.ms = 0.0;
+        cands.push_back(c);
+        int rc = measure(cands.size() - 1);
+        if (rc) {
+            psm_context_set_batch_tuning(ctx, &before);
+            return rc;
+        }
     }
     *best = cands[best_i];
     psm_context_set_batch_tuning(ctx, best);
@@ -1026,7 +1061,7 @@ int psm_match_join_ex(psm_context* ctx, const psm_graph* g, const psm_query_desc
     std::vector<DevResult> dr(U);
     auto run_units = [&](int emit) -> int {
         CK(psm_launch_enum(g->dev, d_uq, U, ctx->d_enum_scratch, d_enum_q, budget, emit, ctx->enum_blocks,
-                           ctx->d_enum_cache, nullptr, 0, ctx->st));
+                           ctx->d_enum_cache, nullptr, 0, ctx->st, 8u, ctx->tune_isect));
         CK(psm_launch_gather(d_uq, U, d_res, ctx->st));
         CK(cudaMemcpyAsync(dr.data(), d_res, sizeof(DevResult) * U, cudaMemcpyDeviceToHost, ctx->st));
         EnumStats es{};

@@ -154,3 +154,207 @@ __device__ __forceinline__ u32 warp_ld_volatile_u32(const u32* p) {
     if ((threadIdx.x & 31u) == 0) v = *(const volatile u32*)p;
     return __shfl_sync(0xffffffffu, v, 0);
 }
+
+// ---- intersections of two ascending arrays of distinct values ----
+//
+// The arrays are table rows (read-only for the kernel: RO = true, loads
+// through __ldg) or the enumerator's cache lists (written by the kernel:
+// plain loads). Values are vertex ids or candidate positions, below
+// 0xFFFFFFFF, which therefore serves as the end-of-array sentinel.
+
+template <bool RO>
+__device__ __forceinline__ u32 ld_sorted(const u32* a, u32 i) {
+    if constexpr (RO)
+        return __ldg(a + i);
+    else
+        return a[i];
+}
+
+template <bool RO>
+__device__ __forceinline__ u32 lower_bound_t(const u32* a, u32 lo, u32 hi, u32 key) {
+    while (lo < hi) {
+        const u32 mid = (lo + hi) >> 1;
+        if (ld_sorted<RO>(a, mid) < key)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ u32 log2_ceil(u32 x) { return x <= 1u ? 0u : 32u - __clz(x - 1u); }
+
+// Intersection variants of the enumerator (psm_batch_tuning::intersect).
+enum : u32 {
+    ISECT_BINARY = 0,  // every entry of the shorter array binary-searched in the longer one
+    ISECT_AUTO = 1,    // per intersection, the variant with the fewer dependent loads
+    ISECT_MERGE = 2,   // merge whenever both arrays are non-empty (for tests of the merge paths)
+};
+
+// Whether a warp intersects arrays of n_short <= n_long entries faster by
+// merge path than by walking the shorter one 32 entries at a time with a
+// binary search of each in the longer one: dependent loads per lane,
+// ceil(n_short / 32) * (log2 n_long + 1) against log2 n_short (the diagonal
+// search) + (n_short + n_long) / 32 (the lane's run) + 3 (its first loads).
+// Balanced arrays merge; an array 16 or more times the other's length is
+// searched.
+__device__ __forceinline__ bool warp_merge_pays(u32 mode, u32 n_short, u32 n_long) {
+    if (mode == ISECT_BINARY || n_short == 0u) return false;
+    if (mode == ISECT_MERGE) return true;
+    const u32 bin = ((n_short + 31u) >> 5) * (log2_ceil(n_long + 1u) + 1u);
+    const u32 mrg = log2_ceil(n_short + 1u) + ((n_short + n_long + 31u) >> 5) + 3u;
+    return mrg < bin;
+}
+
+// The same choice for one lane intersecting on its own: a two-cursor merge
+// (n_short + n_long loads) against a binary search of each entry of the
+// shorter array (n_short * log2 n_long).
+__device__ __forceinline__ bool lane_merge_pays(u32 mode, u32 n_short, u32 n_long) {
+    if (mode == ISECT_BINARY || n_short == 0u) return false;
+    if (mode == ISECT_MERGE) return true;
+    return n_short + n_long < n_short * log2_ceil(n_long + 1u);
+}
+
+// |A ∩ B| by one lane, A the shorter array. A two-cursor merge when
+// lane_merge_pays, else each entry of A searched in B from where the search
+// of the previous entry ended (A ascends, so the range only shrinks).
+template <bool RoA, bool RoB>
+__device__ __forceinline__ u32 lane_isect_count(const u32* A, u32 na, const u32* B, u32 nb, u32 mode) {
+    u32 c = 0;
+    if (na == 0u || nb == 0u) return 0u;
+    if (lane_merge_pays(mode, na, nb)) {
+        u32 i = 0, j = 0;
+        u32 a = ld_sorted<RoA>(A, 0), b = ld_sorted<RoB>(B, 0);
+        while (true) {
+            c += a == b;
+            const bool ta = a <= b, tb = b <= a;
+            if (ta) {
+                if (++i == na) break;
+                a = ld_sorted<RoA>(A, i);
+            }
+            if (tb) {
+                if (++j == nb) break;
+                b = ld_sorted<RoB>(B, j);
+            }
+        }
+        return c;
+    }
+    u32 lo = 0;
+    for (u32 i = 0; i < na; ++i) {
+        const u32 x = ld_sorted<RoA>(A, i);
+        lo = lower_bound_t<RoB>(B, lo, nb, x);
+        if (lo == nb) break;
+        c += ld_sorted<RoB>(B, lo) == x;
+    }
+    return c;
+}
+
+// One lane's run of a merge path (O. Green, R. McColl, D. A. Bader, "GPU
+// merge path: a GPU merging algorithm", ICS 2012): merge steps [k0, k1) of
+// the merge of A[0, na) and B[0, nb) in which, on a tie, A's entry goes
+// first. The run's start (i entries of A and k0 - i of B taken) is found by
+// a binary search along the cross diagonal k0; then the run is walked with
+// one cursor per array. A common value A[i] == B[j] shows as the step that
+// takes B[j] right after A[i]: hit(i, j) is called there, by the lane whose
+// run holds that step, so every common value is seen exactly once.
+template <bool RoA, bool RoB, class Hit>
+__device__ __forceinline__ void merge_run(const u32* A, u32 na, const u32* B, u32 nb, u32 k0, u32 k1, Hit&& hit) {
+    if (k0 >= k1) return;
+    u32 lo = k0 > nb ? k0 - nb : 0u, hi = min(k0, na);
+    while (lo < hi) {
+        const u32 mid = (lo + hi) >> 1;
+        if (ld_sorted<RoA>(A, mid) <= ld_sorted<RoB>(B, k0 - mid - 1u))
+            lo = mid + 1u;
+        else
+            hi = mid;
+    }
+    u32 i = lo, j = k0 - lo;
+    u32 a = i < na ? ld_sorted<RoA>(A, i) : 0xFFFFFFFFu;
+    u32 b = j < nb ? ld_sorted<RoB>(B, j) : 0xFFFFFFFFu;
+    u32 pa = i ? ld_sorted<RoA>(A, i - 1u) : 0xFFFFFFFFu;  // the last entry of A taken
+    for (u32 k = k0; k < k1; ++k) {
+        if (a <= b) {  // B exhausted (b = sentinel) also lands here
+            pa = a;
+            ++i;
+            a = i < na ? ld_sorted<RoA>(A, i) : 0xFFFFFFFFu;
+        } else {
+            if (pa == b) hit(i - 1u, j);
+            ++j;
+            b = j < nb ? ld_sorted<RoB>(B, j) : 0xFFFFFFFFu;
+        }
+    }
+}
+
+// Merge steps per lane and tile of a warp merge path: a tile is 32 runs of
+// at most MERGE_RUN steps; the warp checks a stop flag between tiles.
+constexpr u32 MERGE_RUN = 256;
+
+// Warp-cooperative |A ∩ B| by merge path, counting the common values for
+// which keep(i, j) holds (A[i] == B[j]). With stop non-null, the warp reads
+// *stop between tiles and returns its partial count with *stopped = true
+// once it is set. Called by the whole warp; the result is warp-uniform.
+template <bool RoA, bool RoB, class Keep>
+__device__ u32 warp_merge_count(const u32* A, u32 na, const u32* B, u32 nb, const u32* stop, bool* stopped,
+                                Keep&& keep) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 total = na + nb;
+    const u32 per = min(MERGE_RUN, (total + 31u) >> 5);
+    u32 c = 0;
+    for (u32 t0 = 0; t0 < total; t0 += 32u * per) {
+        if (t0 && stop) {
+            u32 s = 0;
+            if (lane == 0) s = *(const volatile u32*)stop;
+            if (__shfl_sync(0xffffffffu, s, 0)) {
+                *stopped = true;
+                break;
+            }
+        }
+        const u32 k0 = min(total, t0 + lane * per), k1 = min(total, k0 + per);
+        merge_run<RoA, RoB>(A, na, B, nb, k0, k1, [&](u32 i, u32 j) { c += keep(i, j) ? 1u : 0u; });
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    return c;
+}
+
+// Warp-cooperative A ∩ B by merge path, written in ascending order: the
+// common values A[i] for which keep(i) holds go to out[0, n) and n is
+// returned. Each tile is walked twice: once to count every lane's values,
+// once, after the warp has found each lane's offset, to write them. When
+// more than cap values would be written, or with stop non-null *stop is seen
+// set between tiles, *over is set and the count so far is returned. Called
+// by the whole warp; the result is warp-uniform.
+template <bool RoA, bool RoB, class Keep>
+__device__ u32 warp_merge_collect(const u32* A, u32 na, const u32* B, u32 nb, const u32* stop, u32* out, u32 cap,
+                                  bool* over, Keep&& keep) {
+    const u32 lane = threadIdx.x & 31u;
+    const u32 total = na + nb;
+    const u32 per = min(MERGE_RUN, (total + 31u) >> 5);
+    u32 n = 0;
+    for (u32 t0 = 0; t0 < total; t0 += 32u * per) {
+        if (t0 && stop) {
+            u32 s = 0;
+            if (lane == 0) s = *(const volatile u32*)stop;
+            if (__shfl_sync(0xffffffffu, s, 0)) {
+                *over = true;
+                break;
+            }
+        }
+        const u32 k0 = min(total, t0 + lane * per), k1 = min(total, k0 + per);
+        u32 mine = 0;
+        merge_run<RoA, RoB>(A, na, B, nb, k0, k1, [&](u32 i, u32) { mine += keep(i) ? 1u : 0u; });
+        const u32 incl = warp_incl_scan(mine);
+        const u32 tile = __shfl_sync(0xffffffffu, incl, 31);
+        if (n + tile > cap) {
+            *over = true;
+            break;
+        }
+        u32 w = n + incl - mine;
+        merge_run<RoA, RoB>(A, na, B, nb, k0, k1, [&](u32 i, u32) {
+            if (keep(i)) out[w++] = ld_sorted<RoA>(A, i);
+        });
+        n += tile;
+    }
+    return n;
+}
+

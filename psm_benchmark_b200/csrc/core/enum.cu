@@ -220,6 +220,7 @@ __device__ void release_caches(const QState& q, WarpStack* ws) {
 // depth is small enough. Returns false when depth d has no cache plan,
 // caching is off, or the intersection has more than CACHE_CAP entries; the
 // level then intersects the table rows directly.
+template <u32 IS>
 __device__ bool ensure_cache(const QState& q, u32 d, WarpStack* ws, u64& bytes) {
     const u32 cm = q.cmask[d];
     if (cm == 0 || ws->cbuf == nullptr) return false;
@@ -242,15 +243,39 @@ __device__ bool ensure_cache(const QState& q, u32 d, WarpStack* ws, u64& bytes) 
         __syncwarp();
     } else {
         u32 best = 0, blo = 0, blen = 0xFFFFFFFFu, tot = 0;
+        u32 best2 = 0, b2lo = 0, b2len = 0xFFFFFFFFu;
         for (u32 m = cm; m; m &= m - 1) {
             const u32 k = __ffs(m) - 1;
             const u32 lo = row_lo(q, d, k, ws->pos), hi = row_hi(q, d, k, ws->pos);
             tot += hi - lo;
-            if (hi - lo < blen) blen = hi - lo, blo = lo, best = k;
+            if (hi - lo < blen) {
+                b2len = blen, b2lo = blo, best2 = best;
+                blen = hi - lo, blo = lo, best = k;
+            } else if (hi - lo < b2len) {
+                b2len = hi - lo, b2lo = lo, best2 = k;
+            }
         }
         u32* out = slot_list(ws, d);
         const u32 rest = cm & ~(1u << best);
         u32 n = 0;
+        if (IS != ISECT_BINARY && warp_merge_pays(IS, blen, b2len)) {
+            // merge path over the two shortest rows; their common entries
+            // that are in every other row make the list
+            const u32* A = q.adj + blo;
+            const u32 rest2 = rest & ~(1u << best2);
+            n = warp_merge_collect<true, true>(A, blen, q.adj + b2lo, b2len, &q.stop, out, CACHE_CAP, &over,
+                                               [&](u32 i) {
+                                                   const u32 x = __ldg(A + i);
+                                                   for (u32 m = rest2; m; m &= m - 1) {
+                                                       const u32 k = __ffs(m) - 1;
+                                                       if (!contains_u32(q.adj, row_lo(q, d, k, ws->pos),
+                                                                         row_hi(q, d, k, ws->pos), x))
+                                                           return false;
+                                                   }
+                                                   return true;
+                                               });
+            blen = 0;  // the chunked walk below has nothing left to do
+        }
         for (u32 j = 0; j < blen; j += 32) {
             // a stopped query's long intersections end early: the cache is
             // then not kept (the level falls back to the table rows)
@@ -312,9 +337,10 @@ __device__ __forceinline__ bool walk_r_with_bitmap(const WarpStack* ws, u32 d, u
 // reference's intersection of all backward-neighbour rows (8 B of offsets +
 // 4 B per entry each), whether or not a cache saved reading them; returns
 // the driver length.
+template <u32 IS>
 __device__ __forceinline__ u32 setup_level(const QState& q, u32 d, WarpStack* ws, u64& bytes) {
     u32 flg = 0, best = 0, dlo = 0, dhi = 0, olo = 0, ohi = 0;
-    if (ensure_cache(q, d, ws, bytes)) {
+    if (ensure_cache<IS>(q, d, ws, bytes)) {
         const u32 s = ws->clen[d];
         const u32 k = q.crow[d];
         flg = LV_CACHED | LV_DRV_CACHE;
@@ -443,11 +469,12 @@ __device__ __forceinline__ bool chunk_accept(const QState& q, u32 d, u32 p, bool
 }
 
 // Warp-level count of the candidates of the last depth d given the prefix.
+template <u32 IS>
 __device__ u64 count_last(const QState& q, u32 d, WarpStack* ws, u64& bytes, u64& calls) {
     const u32 lane = lane_id();
     const u32 u = q.order[d];
     const u32* list_d = q.list[u];
-    const u32 len = setup_level(q, d, ws, bytes);
+    const u32 len = setup_level<IS>(q, d, ws, bytes);
     calls += len;
     if (len == 0) return 0;
     const u32 f = ws->flg[d];
@@ -475,6 +502,7 @@ __device__ u64 count_last(const QState& q, u32 d, WarpStack* ws, u64& bytes, u64
 
 // Emits the embeddings of the last depth (original data ids, indexed by
 // query vertex) into q.emit_buf; returns how many were found.
+template <u32 IS>
 __device__ u64 emit_last(QState& q, const DevGraph& g, u32 d, WarpStack* ws, u64& bytes, u64& calls) {
     const u32 lane = lane_id();
     const u32 n = d + 1;
@@ -484,7 +512,7 @@ __device__ u64 emit_last(QState& q, const DevGraph& g, u32 d, WarpStack* ws, u64
     // rows emitted so far are the rows counted): a stopped query emits
     // nothing more, and the chunk that crosses the cap is the warp's last.
     if (q.cap && warp_ld_volatile_u32(&q.stop)) return 0;
-    u32 blen = setup_level(q, d, ws, bytes);
+    u32 blen = setup_level<IS>(q, d, ws, bytes);
     calls += blen;
     const u32 bs = ws->cur[d];
     u64 c = 0;
@@ -556,6 +584,7 @@ __device__ __forceinline__ u32 cached_exclusions(const QState& q, u32 dl, u32 v,
     return c;
 }
 
+template <u32 IS>
 __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 v, const WarpStack* ws, u64& bytes,
                                u64& calls, bool* defer, u32 act) {
     const u32 nb = q.nbn[dl];
@@ -590,7 +619,10 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
                 return 0;
             }
             const u32* S = cache_list(q, ws, dl);
-            if (r <= s) {
+            if constexpr (IS != ISECT_BINARY) {
+                c = r <= s ? lane_isect_count<true, false>(q.adj + lo, r, S, s, IS)
+                           : lane_isect_count<false, true>(S, s, q.adj + lo, r, IS);
+            } else if (r <= s) {
                 for (u32 e = lo; e < hi; ++e) c += contains_rw(S, 0, s, __ldg(q.adj + e));
             } else {
                 for (u32 i = 0; i < s; ++i) c += contains_u32(q.adj, lo, hi, S[i]);
@@ -658,6 +690,7 @@ __device__ u64 lane_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
 // the walked side is taken 32 entries at a time, each lane testing its entry
 // against the other arrays. Rows and bytes were counted by the lane that
 // deferred it.
+template <u32 IS>
 __device__ u64 warp_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 v, const WarpStack* ws) {
     const u32 lane = lane_id();
     const u32 nb = q.nbn[dl];
@@ -680,7 +713,11 @@ __device__ u64 warp_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
             }
         } else {
             const u32* S = cache_list(q, ws, dl);
-            if (r <= s) {
+            if (IS != ISECT_BINARY && warp_merge_pays(IS, min(r, s), max(r, s))) {
+                bool st = false;
+                c = warp_merge_count<true, false>(q.adj + lo, r, S, s, &q.stop, &st,
+                                                  [](u32, u32) { return true; });
+            } else if (r <= s) {
                 for (u32 e0 = lo; e0 < hi; e0 += 32) {
                     const u32 e = e0 + lane;
                     const bool ok = e < hi && contains_rw(S, 0, s, __ldg(q.adj + e));
@@ -696,16 +733,46 @@ __device__ u64 warp_last_count(const QState& q, u32 dl, bool cached, u32 p, u32 
         }
         return c - cached_exclusions(q, dl, v, ws, true, lo, hi);
     }
+    // the shortest row drives; the second shortest is its merge partner
     u32 blo = 0, bhi = 0, blen = 0xFFFFFFFFu, bk = 0;
+    u32 b2lo = 0, b2len = 0xFFFFFFFFu, bk2 = 0xFFFFFFFFu;
     for (u32 k = 0; k < nb; ++k) {
         const u32 bd = q.bn_depth[dl][k];
         const u32 base = q.bn_tab[dl][k] + (bd == dp ? p : ws->pos[bd]);
         const u32 lo = q.P[base], hi = q.P[base + 1];
-        if (hi - lo < blen) blen = hi - lo, blo = lo, bhi = hi, bk = k;
+        if (hi - lo < blen) {
+            b2len = blen, b2lo = blo, bk2 = blen == 0xFFFFFFFFu ? 0xFFFFFFFFu : bk;
+            blen = hi - lo, blo = lo, bhi = hi, bk = k;
+        } else if (hi - lo < b2len) {
+            b2len = hi - lo, b2lo = lo, bk2 = k;
+        }
     }
     const u32 u = q.order[dl];
     const u32 same = q.same_mask[dl];
     const u32* list = q.list[u];
+    if (IS != ISECT_BINARY && bk2 != 0xFFFFFFFFu && warp_merge_pays(IS, blen, b2len)) {
+        // merge path over the two shortest rows; each common entry is then
+        // tested against the other rows and the used same-label vertices
+        const u32* A = q.adj + blo;
+        bool st = false;
+        return warp_merge_count<true, true>(A, blen, q.adj + b2lo, b2len, &q.stop, &st, [&](u32 i, u32) {
+            const u32 x = __ldg(A + i);
+            for (u32 k = 0; k < nb; ++k) {
+                if (k == bk || k == bk2) continue;
+                const u32 bd = q.bn_depth[dl][k];
+                const u32 base = q.bn_tab[dl][k] + (bd == dp ? p : ws->pos[bd]);
+                if (!contains_u32(q.adj, q.P[base], q.P[base + 1], x)) return false;
+            }
+            if (same) {
+                const u32 vx = __ldg(list + x);
+                for (u32 m = same; m; m &= m - 1) {
+                    const u32 j = __ffs(m) - 1;
+                    if (vx == (j == dp ? v : ws->vid[j])) return false;
+                }
+            }
+            return true;
+        });
+    }
     u64 c = 0;
     for (u32 e0 = blo; e0 < bhi; e0 += 32) {
         const u32 e = e0 + lane;
@@ -1042,6 +1109,7 @@ __device__ bool periodic(QState& q, u32 qi, WarpStack* ws, u32 d, u32 d0, u32 it
 
 // Depth-first search below the prefix ws->pos[0, d0): the level d0 has been
 // set up (driver range in ws). Returns false if the query stopped.
+template <u32 IS>
 __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws, EnumCtl* ctl, Slot* slots, bool emit,
                     u64& count, u64& bytes, u64& calls, u32& iter) {
     const u32 lane = lane_id();
@@ -1054,7 +1122,7 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
             // The last two depths fused: each lane takes one driver element
             // of depth d and counts its completions at depth d + 1 on its own.
             if (ws->cur[d] < ws->end[d] && q.memo_ok && ((ws->lvfull >> d) & 1u) &&
-                (ws->flg[d] & LV_CACHED) && ((ws->cbits >> d) & 1u) && ensure_cache(q, d + 1, ws, bytes)) {
+                (ws->flg[d] & LV_CACHED) && ((ws->cbits >> d) & 1u) && ensure_cache<IS>(q, d + 1, ws, bytes)) {
                 // the whole level at once through the weight memo
                 const MemoOut mo = memo_count(q, d, ws);
                 count += mo.count;
@@ -1076,20 +1144,20 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
                 bool defer = false;
                 const u32* list_d = q.list[q.order[d]];
                 // the last depth's cache depends on depths <= d - 1 only
-                const bool cached = ensure_cache(q, d + 1, ws, bytes);
+                const bool cached = ensure_cache<IS>(q, d + 1, ws, bytes);
                 const bool valid = idx < end;
                 const u32 p = valid ? (d == 0 ? idx : drv_elem(q, ws, d, idx)) : 0u;
                 const bool ok = d == 0 ? valid : chunk_accept(q, d, p, valid, ws, list_d);
                 const u32 v = ok ? list_d[p] : 0u;
                 const u32 act = __popc(__ballot_sync(FULL_MASK, ok));
-                if (ok) c = lane_last_count(q, d + 1, cached, p, v, ws, bytes_l, calls_l, &defer, act);
+                if (ok) c = lane_last_count<IS>(q, d + 1, cached, p, v, ws, bytes_l, calls_l, &defer, act);
                 count += warp_sum64(c);
                 // long intersections deferred by their lanes: whole warp each
                 u32 dm = __ballot_sync(FULL_MASK, defer);
                 while (dm) {
                     const u32 src = __ffs(dm) - 1;
                     dm &= dm - 1;
-                    count += warp_last_count(q, d + 1, cached, __shfl_sync(FULL_MASK, p, src),
+                    count += warp_last_count<IS>(q, d + 1, cached, __shfl_sync(FULL_MASK, p, src),
                                              __shfl_sync(FULL_MASK, v, src), ws);
                 }
                 calls += min(32u, end - cur);
@@ -1119,10 +1187,10 @@ __device__ bool dfs(const DevGraph& g, QState& q, u32 qi, u32 d0, WarpStack* ws,
             }
             __syncwarp();
             if (d + 2 == n) {
-                count += emit ? emit_last(q, g, d + 1, ws, bytes, calls) : count_last(q, d + 1, ws, bytes, calls);
+                count += emit ? emit_last<IS>(q, g, d + 1, ws, bytes, calls) : count_last<IS>(q, d + 1, ws, bytes, calls);
             } else {
                 d += 1;
-                setup_level(q, d, ws, bytes);
+                setup_level<IS>(q, d, ws, bytes);
             }
         } else if (ws->cur[d] < ws->end[d]) {
             const u32 cur = ws->cur[d], end = ws->end[d];
@@ -1166,6 +1234,7 @@ __device__ void publish(QState& q, u64 count, u64 bytes, u64 calls) {
 }
 
 // Runs one task (prefix positions already in ws->pos[0, d0)).
+template <u32 IS>
 __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpStack* ws, EnumCtl* ctl, Slot* slots,
                          bool emit) {
     const u32 lane = lane_id();
@@ -1225,8 +1294,8 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
             last_r = r;
             __syncwarp();
             // edge pools are built for queries of four or more vertices
-            setup_level(q, 2, ws, bytes);
-            if (!dfs(g, q, t.qi, 2, ws, ctl, slots, emit, count, bytes, calls, iter)) break;
+            setup_level<IS>(q, 2, ws, bytes);
+            if (!dfs<IS>(g, q, t.qi, 2, ws, ctl, slots, emit, count, bytes, calls, iter)) break;
             if (e + 2 < end) try_donate_range(ctl, slots, KIND_EDGES, t.qi, 0, e + 1, end, 0, ws, 2u);
         }
         release_caches(q, ws);
@@ -1239,10 +1308,10 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
     const u32 d0 = t.d0;
     if (t.kind == KIND_FULL && d0 + 1 == n) {
         // donated entry whose children are the last depth
-        count += emit ? emit_last(q, g, d0, ws, bytes, calls) : count_last(q, d0, ws, bytes, calls);
+        count += emit ? emit_last<IS>(q, g, d0, ws, bytes, calls) : count_last<IS>(q, d0, ws, bytes, calls);
     } else {
         if (t.kind == KIND_FULL) {
-            setup_level(q, d0, ws, bytes);
+            setup_level<IS>(q, d0, ws, bytes);
         } else {
             // a donated driver range: rebuild the level the donor had (its
             // cache is a function of the prefix, so the range indexes the
@@ -1252,7 +1321,7 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
             if (flg & LV_CACHED) {
                 // the donor's flags need what the donor had: the cache, and
                 // its bitmap when S is tested through it
-                if (!ensure_cache(q, d0, ws, bytes) || ((flg & LV_OTHER_BM) && !((ws->cbits >> d0) & 1u))) {
+                if (!ensure_cache<IS>(q, d0, ws, bytes) || ((flg & LV_OTHER_BM) && !((ws->cbits >> d0) & 1u))) {
                     if (lane == 0) atomicExch(&ctl->error, 1u);
                     release_caches(q, ws);
                     publish(q, count, bytes, calls);
@@ -1281,7 +1350,7 @@ __device__ void run_task(const DevGraph& g, QState* qs, const TaskHdr& t, WarpSt
             }
             __syncwarp();
         }
-        dfs(g, q, t.qi, d0, ws, ctl, slots, emit, count, bytes, calls, iter);
+        dfs<IS>(g, q, t.qi, d0, ws, ctl, slots, emit, count, bytes, calls, iter);
     }
     release_caches(q, ws);
     publish(q, count, bytes, calls);
@@ -1359,6 +1428,7 @@ __device__ bool take_initial(EnumCtl* ctl, const u32* grab_prefix, const PoolInf
     return true;
 }
 
+template <u32 IS>
 __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 3) enum_kernel(DevGraph g, QState* qs, EnumCtl* ctl,
                                                                     Slot* slots, const u32* grab_prefix,
                                                                     const PoolInfo* pools, int emit, u32* cache) {
@@ -1388,7 +1458,7 @@ __global__ void __launch_bounds__(WARPS_PER_BLOCK * 32, 3) enum_kernel(DevGraph 
             if (hungry && lane == 0) atomicSub(&ctl->hungry, 1u);
             hungry = false;
             spins = 0;
-            run_task(g, qs, t, ws, ctl, slots, emit != 0);
+            run_task<IS>(g, qs, t, ws, ctl, slots, emit != 0);
             ++ntasks;
             __syncwarp();
             if (lane == 0) {
@@ -1557,7 +1627,7 @@ size_t psm_enum_query_bytes(u32 nq) {
 
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
                             int emit, int blocks, u32* cache, QDoneRec* done, u32 exit_keep, cudaStream_t st,
-                            u32 grabs_per_warp) {
+                            u32 grabs_per_warp, u32 isect) {
     EnumCtl* ctl = (EnumCtl*)scratch;
     Slot* slots = (Slot*)((char*)scratch + align16(sizeof(EnumCtl)));
     u32* grab_prefix = (u32*)query_scratch;
@@ -1567,7 +1637,17 @@ cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch
                                          (u32)blocks * WARPS_PER_BLOCK, budget_ns, max(1u, grabs_per_warp));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    enum_kernel<<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, grab_prefix, pools, emit, cache);
+    // one instantiation per intersection variant: the merge paths cost the
+    // binary-search one nothing (registers, instruction cache)
+    if (isect == ISECT_AUTO)
+        enum_kernel<ISECT_AUTO><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, grab_prefix, pools, emit,
+                                                                        cache);
+    else if (isect == ISECT_MERGE)
+        enum_kernel<ISECT_MERGE><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, grab_prefix, pools,
+                                                                         emit, cache);
+    else
+        enum_kernel<ISECT_BINARY><<<blocks, WARPS_PER_BLOCK * 32, 0, st>>>(g, qs, ctl, slots, grab_prefix, pools,
+                                                                          emit, cache);
     return cudaGetLastError();
 }
 
@@ -1577,7 +1657,7 @@ cudaError_t psm_enum_max_blocks(int* blocks) {
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enum_kernel, WARPS_PER_BLOCK * 32, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, enum_kernel<ISECT_BINARY>, WARPS_PER_BLOCK * 32, 0);
     if (e != cudaSuccess) return e;
     *blocks = sms * (per_sm < 1 ? 1 : per_sm);
     return cudaSuccess;

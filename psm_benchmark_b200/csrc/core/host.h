@@ -47,9 +47,13 @@ struct RunInternals {
     int enum_blocks;
     u32 emit;
     u32 prep_status;  // PSM_DEV_* status the run's preparation ended with
+    u32 isect;        // the context's intersection variant (PSM_ISECT_*)
 };
 int psm_run_internals(psm_run* run, RunInternals* out);
 
+// PSM_OK if psm_context_set_batch_tuning would accept t for ctx (reads only
+// the context's fixed launch shape, so any thread may call it).
+int psm_batch_tuning_check(const psm_context* ctx, const psm_batch_tuning* t);
 // Sizes the context's persistent grids to 1/parts of the GPU (serving lanes
 // that run side by side).
 void psm_context_share_gpu(psm_context* ctx, u32 parts);
@@ -93,10 +97,12 @@ size_t psm_enum_cache_bytes(int blocks);
 // completion records in host-mapped memory (device address), or null.
 // exit_keep > 0 lets idle warps beyond that many leave once no work is left.
 // grabs_per_warp: how finely each query's initial work is cut (about that
-// many pieces per warp of the launch for a lone query).
+// many pieces per warp of the launch for a lone query). isect: intersection
+// variant (PSM_ISECT_*: binary search only, by cost per intersection, or
+// merge wherever both arrays are non-empty); each has its own kernel.
 cudaError_t psm_launch_enum(const DevGraph& g, QState* qs, u32 nq, void* scratch, void* query_scratch, u64 budget_ns,
                             int emit, int blocks, u32* cache, QDoneRec* done, u32 exit_keep, cudaStream_t st,
-                            u32 grabs_per_warp = 8);
+                            u32 grabs_per_warp = 8, u32 isect = 0);
 cudaError_t psm_enum_max_blocks(int* blocks);
 cudaError_t psm_launch_gather(const QState* qs, u32 nq, DevResult* out, cudaStream_t st);
 cudaError_t psm_enum_read_ctl(void* scratch, EnumStats* out, cudaStream_t st);

@@ -113,7 +113,7 @@ extern "C" int psm_run_recount_noalloc(psm_run* run, uint64_t cap, double time_l
     e = cudaGetLastError();
     if (e == cudaSuccess)
         e = psm_launch_enum(*ri.dev, ri.dq, 1, scratch, (char*)scratch + ctl_bytes, (u64)(s * 1e9), 0,
-                            ri.enum_blocks, nullptr, nullptr, 0, ri.stream);
+                            ri.enum_blocks, nullptr, nullptr, 0, ri.stream, 8u, ri.isect);
     u64 got = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&got, &ri.dq->count, sizeof(u64), cudaMemcpyDeviceToHost, ri.stream);
     u32 ov = 0;

@@ -54,6 +54,7 @@ struct Request {
 
 struct Lane {
     psm_context* ctx = nullptr;
+    u64 tune_gen = 0;              // the server's tuning generation this lane's context has
     QDoneRec* rec_host = nullptr;  // host-mapped completion records [max_batch]
     QDoneRec* rec_dev = nullptr;
 };
@@ -74,6 +75,8 @@ struct psm_server {
     u64 next_ticket = 1;
     u64 running = 0;
     bool stopping = false;
+    psm_batch_tuning tune{};  // psm_server_set_batch_tuning: applied by each lane before its next batch
+    u64 tune_gen = 0;
 };
 
 namespace {
@@ -162,6 +165,8 @@ void lane_loop(psm_server* s, u32 lane) {
     Lane& ln = s->lanes[lane];
     psm_context* ctx = ln.ctx;
     const u32 keep = s->cfg.lanes > 1 ? (u32)std::max(8, psm_context_enum_warps(ctx) / 16) : 0u;
+    psm_batch_tuning tune{};
+    bool retune = false;
     for (;;) {
         std::vector<Request> batch;
         {
@@ -185,7 +190,15 @@ void lane_loop(psm_server* s, u32 lane) {
             }
             if (batch.empty()) continue;
             s->running += batch.size();
+            if (ln.tune_gen != s->tune_gen) {
+                tune = s->tune;
+                retune = true;
+                ln.tune_gen = s->tune_gen;
+            }
         }
+        // the lane's own thread changes its context's settings, between batches
+        if (retune) psm_context_set_batch_tuning(ctx, &tune);
+        retune = false;
         const u64 t0 = now_ns();
         std::vector<psm_query_desc> qs(batch.size());
         for (size_t i = 0; i < batch.size(); ++i)
@@ -310,6 +323,18 @@ int psm_server_estimate(psm_server* s, const psm_query_desc* q, uint64_t* bytes,
     if (!s || !q || !bytes) return psm_fail(PSM_ERR_ARG, "null argument");
     *bytes = estimate_bytes(*s->g, *q, s->opt, s->prep_blocks);
     if (lane_budget) *lane_budget = s->budget;
+    return PSM_OK;
+}
+
+int psm_server_set_batch_tuning(psm_server* s, const psm_batch_tuning* t) {
+    if (!s || !t) return psm_fail(PSM_ERR_ARG, "null argument");
+    int rc = psm_batch_tuning_check(s->lanes[0].ctx, t);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->tune = *t;
+        s->tune_gen += 1;
+    }
     return PSM_OK;
 }
 

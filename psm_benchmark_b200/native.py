@@ -28,8 +28,9 @@ EXPORTS = [
     "psm_context_set_batch_tuning", "psm_context_get_batch_tuning", "psm_autotune_batch",
     "psm_match_join", "psm_query_decompose", "psm_hash_join", "psm_match_join_ex", "psm_query_decompose_ex",
     "psm_server_create", "psm_server_submit", "psm_server_poll", "psm_server_pending", "psm_server_estimate",
-    "psm_server_clock_ns", "psm_server_destroy",
+    "psm_server_clock_ns", "psm_server_destroy", "psm_server_set_batch_tuning",
     "psm_graph_load_binary", "psm_graph_store_binary", "psm_graph_convert", "psm_graph_convert_edgelist",
+    "psm_intersect_check",
 ]
 MAX_UNITS = 32
 
@@ -74,16 +75,18 @@ class RequestResult(C.Structure):
 
 
 TEAMS = {"RULE": 0, "BLOCK": 1, "CLUSTER": 2}
+INTERSECTS = {"BINARY": 0, "AUTO": 1, "MERGE": 2}
 
 
 class BatchTuning(C.Structure):
     _fields_ = [("team", C.c_uint32), ("grabs_per_warp", C.c_uint32), ("enum_quarters", C.c_uint32),
-                ("reserved", C.c_uint32), ("ms", C.c_double)]
+                ("intersect", C.c_uint32), ("ms", C.c_double)]
 
     def as_dict(self):
         team = {v: k for k, v in TEAMS.items()}[self.team]
+        isect = {v: k for k, v in INTERSECTS.items()}[self.intersect]
         return {"team": team, "grabs_per_warp": self.grabs_per_warp, "enum_quarters": self.enum_quarters,
-                "ms": self.ms}
+                "intersect": isect, "ms": self.ms}
 
 
 SPLIT_PATTERNS = {"BOUNDED": 0, "STAR": 1, "TWINTWIG": 2, "SEED": 3, "SKETCHTREE": 4, "COST": 5}
@@ -152,8 +155,10 @@ def lib():
         "psm_server_estimate": ([vp, C.POINTER(QueryDesc), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
         "psm_server_clock_ns": ([], C.c_uint64),
         "psm_server_destroy": ([vp], None),
+        "psm_server_set_batch_tuning": ([vp, C.POINTER(BatchTuning)], C.c_int),
         "psm_hash_join": ([vp, u32p, C.c_uint64, C.c_uint32, u32p, u32p, C.c_uint64, C.c_uint32, u32p, u32p, u32p,
                            C.c_uint64, u32p, u32p, C.POINTER(C.c_uint64)], C.c_int),
+        "psm_intersect_check": ([u32p, C.c_uint32, u32p, C.c_uint32, C.c_uint32, C.c_uint32, u32p, u32p], C.c_int),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

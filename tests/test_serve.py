@@ -76,3 +76,25 @@ def test_admission_refuses_requests_beyond_the_budget(engine):
     assert res[t_big].status == PSM_ERR_OOM
     assert res[t_small].status == PSM_OK
     assert res[t_small].count == api.match(engine, dg, qs[0], "GQL_GQL_GQL", cap=1000).count
+
+
+def test_server_tuning_reaches_every_lane_and_keeps_counts(engine):
+    """psm_server_set_batch_tuning: the lanes take the setting before their
+    next batch; counts do not change. Out-of-range settings are refused."""
+    from psm_benchmark_b200.native import PsmError
+    g, qs = mixed_queries()
+    dg = api.DataGraph.from_graph(g)
+    cap = 10**6
+    alone = [api.match(engine, dg, q, "CFL_CFL_EXPLORE", cap=cap, time_limit=60).count for q in qs]
+    with api.Server(dg, "CFL_CFL_EXPLORE", cap=cap, time_limit=60, lanes=2, max_batch=8,
+                    lane_arena_bytes=1 << 30) as srv:
+        with pytest.raises(PsmError):
+            srv.set_batch_tuning("BLOCK", 0, 4, "AUTO")
+        for setting in (("BLOCK", 2, 2, "MERGE"), ("BLOCK", 32, 4, "BINARY"), ("RULE", 8, 4, "AUTO")):
+            srv.set_batch_tuning(*setting)
+            tickets = {srv.submit(q): i for i, q in enumerate(qs)}
+            res = srv.drain(len(qs), timeout_s=300)
+            assert len(res) == len(qs)
+            for r in res:
+                assert r.status == PSM_OK
+                assert r.count == alone[tickets[r.ticket]], (setting, tickets[r.ticket])
