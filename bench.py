@@ -426,7 +426,8 @@ def ours_arm(args, world, rank, local):
         line["batched_mixed"] = batched_mixed(args, local, w.graph, dg, flush)
         dg.close()
         line["serve"] = serve_run(args, local)
-    if rank == 0 and args.cpu_baseline and ref_available():
+    if world == 1 and args.cpu_baseline and ref_available():
+        # the host-core baseline runs once, at N = 1 (rank 0 alone)
         line["cpu_baseline"] = cpu_baseline(w, counts, min(args.cpu_queries, nq))
     if rank == 0:
         print(json.dumps(line))
