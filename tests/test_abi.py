@@ -58,3 +58,16 @@ def test_context_without_gpu_fails_cleanly():
     rc = N.lib().psm_context_create(0, 1 << 20, C.byref(h))
     assert rc == N.PSM_ERR_CUDA
     assert N.lib().psm_last_error()
+
+
+def header_defines(prefix: str):
+    text = (ROOT / "include" / "psm_b200.h").read_text()
+    return {m.group(1): int(m.group(2)) for m in re.finditer(rf"#define {prefix}([A-Z]+)\s+(\d+)", text)}
+
+
+def test_binding_constants_match_the_header():
+    """The Python names of the batch settings carry the header's values, and
+    a psm_batch_tuning laid out by the binding has the C struct's size."""
+    assert header_defines("PSM_ISECT_") == N.INTERSECTS
+    assert header_defines("PSM_TEAM_") == N.TEAMS
+    assert C.sizeof(N.BatchTuning) == 4 * 4 + 8
