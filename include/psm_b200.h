@@ -301,8 +301,7 @@ typedef struct psm_server_config {
     uint32_t lanes;             /* concurrent batches: each lane has its own stream, arena, enumerator */
     uint32_t max_batch;         /* queries per batch */
     uint64_t lane_arena_bytes;  /* device arena per lane; requests are admitted within it */
-    uint32_t full_gpu_lanes;    /* 1: each lane's launches may fill most of the GPU (enumeration grids of 3/4
-                                   with several lanes); 0: grids of 1/lanes */
+    uint32_t full_gpu_lanes;    /* 1: every lane's launches may fill the whole GPU; 0: grids of 1/lanes */
     uint32_t reserved;
 } psm_server_config;
 typedef struct psm_request_result {
@@ -332,10 +331,9 @@ int psm_server_pending(psm_server* s, uint64_t* queued, uint64_t* running);
 int psm_server_estimate(psm_server* s, const psm_query_desc* q, uint64_t* bytes, uint64_t* lane_budget);
 uint64_t psm_server_clock_ns(void);
 /* Settings of every lane's batches (psm_batch_tuning, e.g. from
- * psm_autotune_batch on a context of the same device): each lane applies them
- * before its next batch. A server of several whole-GPU lanes starts with
- * enum_quarters = 3 (each enumeration grid 3/4 of the GPU, so the other
- * lanes' small launches find free SMs), otherwise a new context's settings. */
+ * psm_autotune_batch on a context of the same device; enum_quarters < 4 leaves
+ * SMs free for the other lanes' launches): each lane applies them before its
+ * next batch. Lanes start with a new context's settings. */
 int psm_server_set_batch_tuning(psm_server* s, const psm_batch_tuning* t);
 /* Finishes the running batches and stops; queued requests are dropped. */
 void psm_server_destroy(psm_server* s);

@@ -262,15 +262,6 @@ int psm_server_create(int device, const psm_graph* g, const psm_options* opt, co
             return rc;
         }
         if (cfg->lanes > 1 && !cfg->full_gpu_lanes) psm_context_share_gpu(ln.ctx, cfg->lanes);
-        if (cfg->lanes > 1 && cfg->full_gpu_lanes) {
-            // enumeration grids of 3/4 of the GPU: the other lanes' small
-            // launches (preparation, result gather) find free SMs instead of
-            // waiting for a heavy batch's persistent grid to end
-            psm_batch_tuning t{};
-            psm_context_get_batch_tuning(ln.ctx, &t);
-            t.enum_quarters = 3;
-            psm_context_set_batch_tuning(ln.ctx, &t);
-        }
         cudaError_t e = cudaHostAlloc((void**)&ln.rec_host, sizeof(QDoneRec) * cfg->max_batch,
                                       cudaHostAllocMapped | cudaHostAllocPortable);
         if (e == cudaSuccess) e = cudaHostGetDevicePointer((void**)&ln.rec_dev, ln.rec_host, 0);
