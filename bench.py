@@ -331,6 +331,8 @@ def ours_arm(args, world, rank, local):
     from psm_benchmark_b200 import api
     w = make_workload(args)
     eng = api.Engine(device=local, arena_bytes=args.arena_gb << 30)
+    if args.intersect != "BINARY":
+        eng.set_batch_tuning(intersect=args.intersect)
     dg = api.DataGraph.from_graph(w.graph)
     flush = torch.empty(256 << 20 >> 2, dtype=torch.float32, device=f"cuda:{local}")
 
@@ -826,6 +828,8 @@ def main():
     ap.add_argument("--no-legs", dest="legs", action="store_false",
                     help="leave out the batched_mixed and serve keys of the default line")
     ap.add_argument("--only", default="", help="comma-separated query indices (profiling runs)")
+    ap.add_argument("--intersect", default="BINARY", choices=["BINARY", "AUTO", "MERGE"],
+                    help="intersection variant of the plain path's enumeration kernel")
     ap.add_argument("--workload", default="plain", choices=["plain", "batched", "join", "join4", "serve"])
     ap.add_argument("--join-scale", type=int, default=11)
     ap.add_argument("--join-queries", type=int, default=12)
